@@ -1,0 +1,142 @@
+"""ctypes wrapper around oracle/_ref/libcardioid_ref.so: the reference's own
+CPU path (BetterTT06 via ReactionManager, FGRDiffusionOMP, BoxStimulus, the
+omp-loop integrator order of elec/simulationLoop.cc:183-231) compiled from the
+reference sources by oracle/ref/Makefile.
+
+TEST INFRASTRUCTURE.  Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline use it, as the checker; the product never imports it.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+REF_LIB = os.path.join(REF_DIR, "libcardioid_ref.so")
+REF_SINGLECELL = os.path.join(REF_DIR, "singleCell")
+
+_lib = None
+
+
+def available():
+    return os.path.exists(REF_LIB)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not available():
+            raise RuntimeError("oracle/_ref is not built (make -C oracle/ref)")
+        L = ctypes.CDLL(REF_LIB, mode=ctypes.RTLD_LOCAL)
+        vp, dp, ip, lp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_longlong)
+        L.ref_objects_compile.argtypes = [ctypes.c_char_p]
+        L.ref_sim_create.restype = vp
+        L.ref_sim_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_long, lp, ip, dp,
+                                     ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.ref_sim_destroy.argtypes = [vp]
+        L.ref_sim_ncells.argtypes = [vp]
+        L.ref_sim_ncells.restype = ctypes.c_long
+        L.ref_sim_time.argtypes = [vp]
+        L.ref_sim_time.restype = ctypes.c_double
+        L.ref_sim_get_vm.argtypes = [vp, dp]
+        L.ref_sim_set_vm.argtypes = [vp, dp]
+        L.ref_sim_get_dvm.argtypes = [vp, dp, dp, dp]
+        L.ref_sim_get_activation.argtypes = [vp, dp]
+        L.ref_sim_field_names.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+        L.ref_sim_get_state.argtypes = [vp, ctypes.c_char_p, dp]
+        L.ref_sim_set_state.argtypes = [vp, ctypes.c_char_p, dp]
+        L.ref_sim_step.argtypes = [vp, ctypes.c_int]
+        L.ref_set_threads.argtypes = [ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def compile_objects(text):
+    lib().ref_objects_compile(text.encode())
+
+
+class RefSim:
+    """One tissue on the reference CPU path.  Cells in local order (gid
+    order for the synthetic boxes)."""
+
+    def __init__(self, reactions, stimuli, grid, spacing, gid, cell_type, sigma6, dt,
+                 diffusion_scale, diffusion=True):
+        L = lib()
+        self.n = len(gid)
+        self._gid = np.ascontiguousarray(gid, dtype=np.int64)
+        self._ct = np.ascontiguousarray(cell_type, dtype=np.int32)
+        self._sig = np.ascontiguousarray(sigma6, dtype=np.float64).reshape(-1)
+        nx, ny, nz = grid
+        dx, dy, dz = spacing
+        self.h = L.ref_sim_create(" ".join(reactions).encode(), " ".join(stimuli).encode(),
+                                  nx, ny, nz, dx, dy, dz, self.n,
+                                  self._gid.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                                  self._ct.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                  _dp(self._sig), dt, diffusion_scale, 1 if diffusion else 0)
+        if not self.h:
+            raise RuntimeError("ref_sim_create failed")
+
+    def close(self):
+        if self.h:
+            lib().ref_sim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n=1):
+        lib().ref_sim_step(self.h, n)
+
+    @property
+    def time(self):
+        return lib().ref_sim_time(self.h)
+
+    def vm(self):
+        out = np.empty(self.n)
+        lib().ref_sim_get_vm(self.h, _dp(out))
+        return out
+
+    def set_vm(self, vm):
+        v = np.ascontiguousarray(vm, dtype=np.float64)
+        lib().ref_sim_set_vm(self.h, _dp(v))
+
+    def dvm(self):
+        r, d, s = np.empty(self.n), np.empty(self.n), np.empty(self.n)
+        lib().ref_sim_get_dvm(self.h, _dp(r), _dp(d), _dp(s))
+        return r, d, s
+
+    def activation(self):
+        out = np.empty(self.n)
+        lib().ref_sim_get_activation(self.h, _dp(out))
+        return out
+
+    def field_names(self):
+        buf = ctypes.create_string_buffer(4096)
+        n = lib().ref_sim_field_names(self.h, buf, 4096)
+        if n < 0:
+            raise RuntimeError("field name buffer too small")
+        return buf.value.decode().split()
+
+    def state(self, name):
+        out = np.empty(self.n)
+        if lib().ref_sim_get_state(self.h, name.encode(), _dp(out)) != 0:
+            raise KeyError(name)
+        return out
+
+    def set_state(self, name, values):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        if lib().ref_sim_set_state(self.h, name.encode(), _dp(v)) != 0:
+            raise KeyError(name)
+
+
+def set_threads(n):
+    lib().ref_set_threads(int(n))
