@@ -1,0 +1,340 @@
+"""Benchmark of the fused monodomain step: cell-steps/s on the 256^3 box
+(BetterTT06 + FGR 19-point stencil + face pacing, dt = 0.02 ms), mixed
+FP32/FP64 (headline) and FP64, one fused kernel per time step.
+
+    python bench.py [--gpus N --steps K --warmup W]       # our engine
+    python bench.py --impl reference [...]                 # the reference CPU path
+
+One process per GPU (torchrun for N > 1); each GPU runs its own 256^3 tissue
+(independent tissues shard with no data-path collective: weak scaling).
+Prints one JSON line on rank 0.
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT = 0.02
+METRIC = "cell-steps/s"
+# algorithmic bytes per cell-step of one fused step (compulsory HBM traffic):
+# Vm read+write 16 B; state FP64 18x8x2 = 288 B, mixed 5x8x2 + 13x4x2 = 184 B;
+# stencil weights FP64 19x8 = 152 B, mixed 18x4 = 72 B; reaction byte 1 B.
+ALGO_BYTES = {"fp64": 16 + 288 + 152 + 1, "mixed": 16 + 184 + 72 + 1}
+CPU_SAMPLE = (64, 64, 32)     # cells per CPU worker process
+
+
+def workload(name):
+    if name == "box256":
+        return dict(nx=256, ny=256, nz=256, period=500.0, label="box256: 256^3 = 16,777,216 cells, dx 0.2 mm, "
+                    "endo/mid/epi x-slabs 25/35/40 %, fibre -60..+60 deg across z, sigma_l 0.133 / sigma_t 0.0176 S/m, "
+                    "beta 1400/cm, Cm 1 uF/cm^2, S1 pacing every 500 ms on the x = 0 face, dt 0.02 ms")
+    if name == "box64":
+        return dict(nx=64, ny=64, nz=64, period=1000.0, label="box64: 64^3 = 262,144 cells, single stimulus at t = 0 "
+                    "on the x = 0 face, otherwise as box256")
+    raise ValueError(name)
+
+
+def read_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (6.65 TB/s)"
+
+
+def read_traffic(precision):
+    """DRAM bytes per cell-step of the fused kernel from the committed ncu
+    summary (profiles/fused_step_traffic.json), if one exists."""
+    path = os.path.join(ROOT, "profiles", "fused_step_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    v = d.get(precision, {}).get("dram_bytes_per_cell_step")
+    return float(v) if v is not None else None
+
+
+# ---------------------------------------------------------------- CPU side
+
+def _cpu_worker(args):
+    """Runs the reference CPU path (oracle/_ref) or the oracle port on one
+    sample box; returns (cells, steps, seconds)."""
+    kind, shape, steps, warmup, seed = args
+    os.environ["OMP_NUM_THREADS"] = "1"
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from cardioid_b200 import engine, tissue
+    t = tissue.box(*shape, seed=seed)
+    if kind == "reference":
+        from golden.make_golden import reference_sim
+        from oracle import refsim
+        refsim.set_threads(1)
+        sim = reference_sim(t)
+        sim.set_vm(t.vm0)
+    else:
+        from oracle import port
+        params = [engine.default_params(ct, DT) for ct in (0, 1, 2)]
+        sim = port.PortSim(t, params, (t.cell_type - 100).astype(np.uint8), DT)
+    sim.step(warmup)
+    t0 = time.perf_counter()
+    sim.step(steps)
+    return t.n, steps, time.perf_counter() - t0
+
+
+def cpu_baseline(steps, warmup, procs=None):
+    from oracle import refsim
+    kind = "reference" if refsim.available() else "port"
+    procs = procs or os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_cpu_worker, [(kind, CPU_SAMPLE, steps, warmup, 100 + i) for i in range(procs)])
+    cells = sum(r[0] * r[1] for r in res)
+    wall = max(r[2] for r in res)
+    cpu = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    cpu = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    what = ("the reference's own CPU path (oracle/_ref: BetterTT06 + FGRDiffusionOMP + BoxStimulus, omp-loop order)"
+            if kind == "reference" else "the oracle's C restatement of the reference path")
+    return {"value": cells / wall, "unit": METRIC, "cores": procs, "kind": kind,
+            "sample": "%s; %d processes (one per host core, like one MPI rank per core, no halo exchange), "
+                      "each a %dx%dx%d box of the same workload for %d steps after %d warm-up; CPU: %s"
+                      % (what, procs, CPU_SAMPLE[0], CPU_SAMPLE[1], CPU_SAMPLE[2], steps, warmup, cpu)}
+
+
+# ---------------------------------------------------------------- clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- GPU side
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=__import__("torch").device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world, local):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda:%d" % local)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_engine(e, steps, warmup, world, local):
+    import torch
+    stream = torch.cuda.ExternalStream(e.stream(), device="cuda:%d" % local)
+    e.step(warmup)
+    e.sync()
+    torch.cuda.synchronize(local)
+    barrier(world)
+    l0 = e.launch_count()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        e.step(steps)
+        stop.record(stream)
+        stop.synchronize()
+    torch.cuda.synchronize(local)
+    ms = start.elapsed_time(stop)
+    barrier(world)
+    return ms, e.launch_count() - l0, clk.summary()
+
+
+def run_ours(args):
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from cardioid_b200 import engine, tissue
+    w = workload(args.config)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(args.cpu_steps, 2)          # before the first GPU call
+    t = tissue.box(w["nx"], w["ny"], w["nz"], period=w["period"], seed=1234 + rank)
+    n = t.n
+    peak, peak_src = read_peaks()
+    results = {}
+    for prec in ("fp64", "mixed"):
+        with engine.Engine(DT, precision=prec, device=local) as e:
+            rx, _ = engine.transmural_setup(e, t, DT)
+            e.add_tissue(t, rx)
+            ms, launches, clocks = time_engine(e, args.steps, args.warmup, world, local)
+            ms = max_over_ranks(ms, world, local)
+            per_launch_s = ms / 1e3 / args.steps
+            achieved = ALGO_BYTES[prec] * n / per_launch_s / 1e9
+            traffic_pc = read_traffic(prec)
+            results[prec] = {
+                "value": world * n * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                "gpu_launches": launches, "clocks": clocks,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_source": peak_src,
+                             "algorithmic_bytes_per_cell_step": ALGO_BYTES[prec],
+                             "traffic": (traffic_pc * n if traffic_pc else None)},
+            }
+            if prec == "mixed":
+                # end to end through the C ABI with host buffers: every step
+                # copies Vm in from pinned host memory and the new Vm back
+                vin = torch.from_numpy(t.vm0.copy()).pin_memory()
+                vout = torch.empty_like(vin).pin_memory()
+                vin_np, vout_np = vin.numpy(), vout.numpy()
+                e2e_steps = max(1, min(args.steps, args.e2e_steps))
+                for _ in range(args.warmup):
+                    e.step_host(0, vin_np, vout_np)
+                barrier(world)
+                t0 = time.perf_counter()
+                for _ in range(e2e_steps):
+                    e.step_host(0, vin_np, vout_np)
+                    vin_np, vout_np = vout_np, vin_np
+                el = max_over_ranks(time.perf_counter() - t0, world, local)
+                results["e2e"] = {"value": world * n * e2e_steps / el, "unit": METRIC,
+                                  "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n,
+                                  "steps": e2e_steps,
+                                  "call": "cdb_engine_step_host (pinned host Vm in, one fused step, host Vm out)"}
+    if rank != 0:
+        return
+    m, f = results["mixed"], results["fp64"]
+    line = {
+        "metric": METRIC, "value": m["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64 (mixed: FP32 fits/gates/currents/stencil, FP64 Vm and concentrations)",
+        "data": "synthetic, seeded (no dataset: the configs define geometry, fibres and pacing)",
+        "config": {"workload": w["label"], "cells_per_gpu": n, "dt_ms": DT, "precision": "mixed",
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (state + weights %.1f GB per GPU)" % (
+                       (ALGO_BYTES["mixed"] - 16) * n / 1e9)},
+        "impl": "ours",
+        "roofline": m["roofline"],
+        "fp64": {"value": f["value"], "ms_per_step": f["ms_per_step"], "roofline": f["roofline"],
+                 "dtype": "f64"},
+        "mixed_over_fp64": m["value"] / f["value"],
+        "e2e": results["e2e"],
+        "gpu_launches": m["gpu_launches"],
+        "clocks": m["clocks"],
+        "clocks_fp64": f["clocks"],
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = workload(args.config)
+    cb = cpu_baseline(args.steps, args.warmup)
+    line = {
+        "metric": METRIC, "value": cb["value"], "unit": METRIC, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic, seeded",
+        "config": {"workload": w["label"], "precision": "fp64 (reference CPU path)"},
+        "impl": "reference",
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=["box256", "box64"], default="box256")
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,134 @@
+// Shared host/device plumbing of the cardioid_b200 library: error status,
+// device allocations, reaction-type tables in constant memory.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <string>
+
+#include "../../include/cardioid_b200.h"
+#include "tt06_device.cuh"
+
+namespace cdb {
+
+constexpr int kFitPoolPerType = 640;   // coefficients of one reaction type's 30 fits
+static_assert(kMaxReactionTypes >= CDB_MAX_REACTION_TYPES, "type table size");
+
+void set_error(const std::string& msg);
+
+// Reaction-type tables, uploaded once per type (constant memory: every
+// thread of a warp reads the same coefficient).
+struct TypeTables {
+  TT06Scalars scal[CDB_MAX_REACTION_TYPES];
+  FitShape shape[CDB_MAX_REACTION_TYPES];
+};
+
+struct Status {
+  cdb_status code = CDB_OK;
+  bool ok() const { return code == CDB_OK; }
+};
+
+#define CDB_CUDA(call)                                                                     \
+  do {                                                                                     \
+    cudaError_t _e = (call);                                                               \
+    if (_e != cudaSuccess) {                                                               \
+      ::cdb::set_error(std::string(#call) + ": " + cudaGetErrorString(_e));                \
+      return (_e == cudaErrorMemoryAllocation) ? CDB_OOM : CDB_CUDA_ERROR;                 \
+    }                                                                                      \
+  } while (0)
+
+#define CDB_CHECK(cond, code, msg)                                                         \
+  do {                                                                                     \
+    if (!(cond)) {                                                                         \
+      ::cdb::set_error(msg);                                                               \
+      return code;                                                                         \
+    }                                                                                      \
+  } while (0)
+
+// Packs 30 fits into a coefficient pool; fails when they do not fit.
+inline bool pack_fits(const cdb_fit* fits, FitShape& sh, double* pool, int poolSize, std::string& err)
+{
+  int off = 0;
+  for (int f = 0; f < kNumFits; ++f) {
+    const int nn = fits[f].numer, nd = fits[f].denom;
+    if (nn < 1 || nd < 1 || nn + nd - 1 > CDB_MAX_COEFF) {
+      err = "fit " + std::to_string(f) + " has invalid term counts";
+      return false;
+    }
+    if (off + nn + nd - 1 > poolSize) {
+      err = "fits of one reaction type exceed " + std::to_string(poolSize) + " coefficients";
+      return false;
+    }
+    sh.numer[f] = (int16_t)nn;
+    sh.denom[f] = (int16_t)nd;
+    sh.offset[f] = (int16_t)off;
+    for (int k = 0; k < nn + nd - 1; ++k) pool[off + k] = fits[f].coeff[k];
+    off += nn + nd - 1;
+  }
+  return true;
+}
+
+inline TT06Scalars to_scalars(const cdb_tt06_params& p)
+{
+  TT06Scalars s;
+  s.celltype = p.celltype; s.g_CaL = p.g_CaL; s.g_K1 = p.g_K1; s.g_Kr = p.g_Kr; s.g_Ks = p.g_Ks;
+  s.g_Na = p.g_Na; s.g_bca = p.g_bca; s.g_bna = p.g_bna; s.g_pCa = p.g_pCa; s.g_pK = p.g_pK; s.g_to = p.g_to;
+  return s;
+}
+
+// Initial state of BetterTT06 (initializeMembraneVoltage, elec/BetterTT06.cc:1657-1712),
+// checkpoint order.
+__host__ __device__ inline double tt06_initial_state(int k)
+{
+  switch (k) {
+    case S_Ca_SR: return 3.155;
+    case S_Ca_i: return 2.0e-5;
+    case S_Ca_ss: return 0.00017;
+    case S_K_i: return 138.4;
+    case S_Na_i: return 10.355;
+    case S_R_prime: return 0.9868;
+    case S_Xr1: return 0.00448;
+    case S_Xr2: return 0.476;
+    case S_Xs: return 0.0087;
+    case S_d: return 3.164e-5;
+    case S_f: return 0.9609;
+    case S_f2: return 0.9778;
+    case S_fCass: return 0.9953;
+    case S_h: return 0.55;
+    case S_j: return 0.66;
+    case S_m: return 0.00155;
+    case S_r: return 2.235e-8;
+    default: return 0.6012;   // s
+  }
+}
+constexpr double kInitialVm = -83.0;
+
+// Order-preserving map of doubles onto unsigned 64-bit integers, for
+// atomicMin / atomicMax reductions.
+__host__ __device__ inline unsigned long long ordered_bits(double v)
+{
+#ifdef __CUDA_ARCH__
+  long long b = __double_as_longlong(v);
+#else
+  long long b;
+  std::memcpy(&b, &v, 8);
+#endif
+  return b >= 0 ? (unsigned long long)b ^ 0x8000000000000000ull : ~(unsigned long long)b;
+}
+__host__ __device__ inline double from_ordered_bits(unsigned long long u)
+{
+  unsigned long long b = (u & 0x8000000000000000ull) ? (u ^ 0x8000000000000000ull) : ~u;
+  double v;
+#ifdef __CUDA_ARCH__
+  v = __longlong_as_double((long long)b);
+#else
+  std::memcpy(&v, &b, 8);
+#endif
+  return v;
+}
+
+// Device-side counter of launches made by this library (for reporting).
+extern int64_t g_launches;
+
+}  // namespace cdb

@@ -1,0 +1,1082 @@
+// Fused monodomain engine: one kernel per time step does, for every tissue
+// cell, the FGR stencil on Vm(t), the BetterTT06 update, the box stimuli,
+// the integrator Vm(t+dt) = Vm + dt (dVmR + dVmD + iStim) and the sensors
+// (activation time, min/max Vm), in the order of the reference's omp loop
+// (elec/simulationLoop.cc:183-231), reading Vm from one buffer and writing
+// the other so Vm crosses HBM once per step.
+//
+// HBM layout, per tissue (all arrays separate cudaMalloc allocations, so
+// tissues join and retire between steps without moving anyone else):
+//   vm[2]      padded Vm blocks (halo of one voxel, zero, never written)
+//              in x-fastest order; only dimensions longer than one voxel
+//              are padded (a cable is nx+2 long, a sheet (nx+2)(ny+2));
+//   s64, s32   state, structure of arrays with pitch n: FP64 path 18 rows
+//              of double; mixed path 5 rows of double (Ca_SR Ca_i Ca_ss K_i
+//              Na_i) and 13 of float (R_prime and the 12 gates);
+//   w          stencil weights, rows x n (FP64: A0 and the class's nodes in
+//              double; mixed: the class's nodes without A0 in float);
+//   rtype      reaction-type byte per cell; voxel (masked tissues only)
+//              int64 padded-voxel index per cell; act activation time.
+// A tile table maps each CTA to kTile consecutive cells of one tissue.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "fgr_device.cuh"
+
+namespace cdb {
+
+thread_local std::string t_last_error;
+void set_error(const std::string& msg) { t_last_error = msg; }
+int64_t g_launches = 0;
+
+constexpr int kTile = 128;
+
+__constant__ TT06Scalars c_scal[CDB_MAX_REACTION_TYPES];
+__constant__ FitShape c_shape[CDB_MAX_REACTION_TYPES];
+__constant__ double c_coef64[CDB_MAX_REACTION_TYPES * kFitPoolPerType];
+__constant__ float c_coef32[CDB_MAX_REACTION_TYPES * kFitPoolPerType];
+
+struct TissueDev {
+  double* vm[2];
+  double* s64;
+  float* s32;
+  const void* w;
+  const uint8_t* rtype;
+  const int64_t* voxel;
+  double* act;
+  int64_t n;
+  int64_t px, pxy;        // padded strides
+  int nx, ny, nz;
+  int py0, pz0;           // 1 when y (z) is padded
+  int cls;
+  int nstim, stim0;
+  int parity;             // buffer holding Vm at the start of the next launch batch
+  int64_t step0;          // steps taken at the start of the next launch batch
+  double scale;           // diffusionScale (0: no diffusion)
+  BlockScale blk;
+  unsigned long long* minmax;   // 2 slots
+};
+
+struct Tile {
+  int tissue;
+  int count;
+  int64_t first;
+};
+
+struct StepArgs {
+  TissueDev* tissues;
+  const Tile* tiles;
+  const cdb_stimulus* stims;
+  const double* times;
+  double dt;
+  int k;                  // step within the launch batch
+  int minmax;             // reduce min/max this step
+};
+
+__device__ __forceinline__ double pulse_value(const cdb_stimulus& s, double time)
+{
+  if (!(time > s.t0 && time < s.tf)) return 0.0;
+  const double t = time - floor(time / s.period) * s.period;
+  return (t >= s.phase && t < s.phase + s.duration) ? s.amplitude : 0.0;
+}
+
+// Geometry of one tissue, held in registers by the step kernel.
+struct Geom {
+  const int64_t* voxel;
+  int64_t px, pxy;
+  int nx, ny, py0, pz0;
+};
+
+__device__ __forceinline__ void cell_coords(const Geom& g, int64_t i, int64_t& vox, int& x, int& y, int& z)
+{
+  if (g.voxel) {
+    vox = g.voxel[i];
+    const int64_t yz = vox / g.px;
+    x = (int)(vox - yz * g.px) - 1;
+    const int64_t py = g.pxy / g.px;
+    const int64_t zz = yz / py;
+    y = (int)(yz - zz * py) - g.py0;
+    z = (int)zz - g.pz0;
+  } else {
+    const int nxy = g.nx * g.ny;
+    const int ii = (int)i;
+    z = ii / nxy;
+    const int r = ii - z * nxy;
+    y = r / g.nx;
+    x = r - y * g.nx;
+    vox = (int64_t)(x + 1) + g.px * (int64_t)(y + g.py0) + g.pxy * (int64_t)(z + g.pz0);
+  }
+}
+
+__device__ __forceinline__ int64_t node_offset(int64_t px, int64_t pxy, int node)
+{
+  return (int64_t)node_dx(node) + px * node_dy(node) + pxy * node_dz(node);
+}
+
+// FP64 stencil in the reference's order: A0 phi0 + sum_k A_k phi_k.
+template <int CLS>
+__device__ __forceinline__ double stencil64(const double* __restrict__ w, int64_t n, int64_t px, int64_t pxy,
+                                            const double* __restrict__ vin, int64_t vox, double phi0, int64_t i)
+{
+  double tmp = __ldg(w + i) * phi0;
+#pragma unroll
+  for (int r = 1; r < class_rows(CLS); ++r) {
+    const int node = class_node(CLS, r);
+    tmp += __ldg(w + r * n + i) * __ldg(vin + vox + node_offset(px, pxy, node));
+  }
+  return tmp;
+}
+
+// Mixed stencil: sum_k A_k (phi_k - phi0) with FP32 weights; the
+// differences are taken in FP64 (A0 = -sum A_k).
+template <int CLS>
+__device__ __forceinline__ double stencil32(const float* __restrict__ w, int64_t n, int64_t px, int64_t pxy,
+                                            const double* __restrict__ vin, int64_t vox, double phi0, int64_t i)
+{
+  float tmp = 0.f;
+#pragma unroll
+  for (int r = 1; r < class_rows(CLS); ++r) {
+    const int node = class_node(CLS, r);
+    const float d = (float)(__ldg(vin + vox + node_offset(px, pxy, node)) - phi0);
+    tmp = fmaf(__ldg(w + (r - 1) * n + i), d, tmp);
+  }
+  return (double)tmp;
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(kTile) fused_step_kernel(StepArgs a)
+{
+  __shared__ cdb_stimulus s_stim[CDB_MAX_STIM_PER_TISSUE];
+  __shared__ double s_val[CDB_MAX_STIM_PER_TISSUE];
+  const Tile tile = a.tiles[blockIdx.x];
+  const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
+  const int64_t lstep = Tp->step0 + a.k;
+  const double time = a.times[lstep];
+  const double tnext = a.times[lstep + 1];
+  const int nstim = Tp->nstim;
+  if (threadIdx.x < nstim) {
+    s_stim[threadIdx.x] = a.stims[Tp->stim0 + threadIdx.x];
+    s_val[threadIdx.x] = pulse_value(s_stim[threadIdx.x], time);
+  }
+  __syncthreads();
+  const bool active = threadIdx.x < tile.count;
+  double vnew = 0.0;
+  if (active) {
+    const int64_t i = tile.first + threadIdx.x;
+    const int cur = (Tp->parity + a.k) & 1;
+    const double* __restrict__ vin = Tp->vm[cur];
+    double* __restrict__ vout = Tp->vm[cur ^ 1];
+    Geom g;
+    g.voxel = Tp->voxel; g.px = Tp->px; g.pxy = Tp->pxy; g.nx = Tp->nx; g.ny = Tp->ny;
+    g.py0 = Tp->py0; g.pz0 = Tp->pz0;
+    const int64_t n = Tp->n;   // tissues hold fewer than 2^31 cells
+    const double scale = Tp->scale;
+    const int cls = Tp->cls;
+    const void* wp = Tp->w;
+    const BlockScale blk = Tp->blk;
+    double* const s64base = Tp->s64;
+    float* const s32base = Tp->s32;
+    double* const act = Tp->act;
+    const int rt = Tp->rtype[i];
+    int64_t vox;
+    int x, y, z;
+    cell_coords(g, i, vox, x, y, z);
+    const double phi0 = vin[vox];
+
+    double dvmD = 0.0;
+    if (scale != 0.0) {
+      double acc;
+      if (MIXED) {
+        const float* w = (const float*)wp;
+        acc = cls == kVolume ? stencil32<kVolume>(w, n, g.px, g.pxy, vin, vox, phi0, i)
+            : cls == kSheet ? stencil32<kSheet>(w, n, g.px, g.pxy, vin, vox, phi0, i)
+                            : stencil32<kCable>(w, n, g.px, g.pxy, vin, vox, phi0, i);
+      } else {
+        const double* w = (const double*)wp;
+        acc = cls == kVolume ? stencil64<kVolume>(w, n, g.px, g.pxy, vin, vox, phi0, i)
+            : cls == kSheet ? stencil64<kSheet>(w, n, g.px, g.pxy, vin, vox, phi0, i)
+                            : stencil64<kCable>(w, n, g.px, g.pxy, vin, vox, phi0, i);
+      }
+      dvmD = acc * scale;
+    }
+
+    double dvmR;
+    if (MIXED) {
+      double* s64 = s64base + i;
+      float* s32 = s32base + i;
+      CellState<float> st;
+      st.caSR = s64[0 * n]; st.caI = s64[1 * n]; st.caSS = s64[2 * n];
+      st.kI = s64[3 * n]; st.naI = s64[4 * n];
+      st.rPrime = s32[0 * n]; st.Xr1 = s32[1 * n]; st.Xr2 = s32[2 * n];
+      st.Xs = s32[3 * n]; st.d = s32[4 * n]; st.f = s32[5 * n];
+      st.f2 = s32[6 * n]; st.fCass = s32[7 * n]; st.h = s32[8 * n];
+      st.j = s32[9 * n]; st.m = s32[10 * n]; st.r = s32[11 * n];
+      st.s = s32[12 * n];
+      dvmR = (double)tt06_step_mixed(c_scal[rt], blk, c_coef32 + rt * kFitPoolPerType, c_shape[rt],
+                                     (float)a.dt, a.dt, phi0, st);
+      s64[0 * n] = st.caSR; s64[1 * n] = st.caI; s64[2 * n] = st.caSS;
+      s64[3 * n] = st.kI; s64[4 * n] = st.naI;
+      s32[0 * n] = st.rPrime; s32[1 * n] = st.Xr1; s32[2 * n] = st.Xr2;
+      s32[3 * n] = st.Xs; s32[4 * n] = st.d; s32[5 * n] = st.f;
+      s32[6 * n] = st.f2; s32[7 * n] = st.fCass; s32[8 * n] = st.h;
+      s32[9 * n] = st.j; s32[10 * n] = st.m; s32[11 * n] = st.r;
+      s32[12 * n] = st.s;
+    } else {
+      double* s = s64base + i;
+      CellState<double> st;
+      st.caSR = s[S_Ca_SR * n]; st.caI = s[S_Ca_i * n]; st.caSS = s[S_Ca_ss * n];
+      st.kI = s[S_K_i * n]; st.naI = s[S_Na_i * n]; st.rPrime = s[S_R_prime * n];
+      st.Xr1 = s[S_Xr1 * n]; st.Xr2 = s[S_Xr2 * n]; st.Xs = s[S_Xs * n];
+      st.d = s[S_d * n]; st.f = s[S_f * n]; st.f2 = s[S_f2 * n];
+      st.fCass = s[S_fCass * n]; st.h = s[S_h * n]; st.j = s[S_j * n];
+      st.m = s[S_m * n]; st.r = s[S_r * n]; st.s = s[S_s * n];
+      dvmR = tt06_step(c_scal[rt], blk, c_coef64 + rt * kFitPoolPerType, c_shape[rt], a.dt, phi0, st);
+      s[S_Ca_SR * n] = st.caSR; s[S_Ca_i * n] = st.caI; s[S_Ca_ss * n] = st.caSS;
+      s[S_K_i * n] = st.kI; s[S_Na_i * n] = st.naI; s[S_R_prime * n] = st.rPrime;
+      s[S_Xr1 * n] = st.Xr1; s[S_Xr2 * n] = st.Xr2; s[S_Xs * n] = st.Xs;
+      s[S_d * n] = st.d; s[S_f * n] = st.f; s[S_f2 * n] = st.f2;
+      s[S_fCass * n] = st.fCass; s[S_h * n] = st.h; s[S_j * n] = st.j;
+      s[S_m * n] = st.m; s[S_r * n] = st.r; s[S_s * n] = st.s;
+    }
+
+    double istim = 0.0;
+    for (int k = 0; k < nstim; ++k) {
+      const double v = s_val[k];
+      if (v != 0.0) {
+        const cdb_stimulus& b = s_stim[k];
+        if (x > b.xMin && x < b.xMax && y > b.yMin && y < b.yMax && z > b.zMin && z < b.zMax) istim = v;
+      }
+    }
+    vnew = phi0 + a.dt * (dvmR + dvmD + istim);
+    vout[vox] = vnew;
+    if (vnew > 0.0) {
+      double* ap = act + i;
+      if (*ap < 0.0) *ap = tnext;
+    }
+  }
+  if (a.minmax) {
+    double lo = active ? vnew : __longlong_as_double(0x7ff0000000000000ll);
+    double hi = active ? vnew : -__longlong_as_double(0x7ff0000000000000ll);
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((threadIdx.x & 31) == 0 && (threadIdx.x < tile.count)) {
+      atomicMin(Tp->minmax, ordered_bits(lo));
+      atomicMax(Tp->minmax + 1, ordered_bits(hi));
+    }
+  }
+}
+
+// After a launch batch of k steps: every tissue is k steps further.
+__global__ void advance_kernel(TissueDev* tissues, int nTissues, int k)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nTissues) {
+    tissues[t].step0 += k;
+    tissues[t].parity = (tissues[t].parity + k) & 1;
+  }
+}
+
+__global__ void reset_minmax_kernel(TissueDev* tissues, int nTissues)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nTissues) {
+    tissues[t].minmax[0] = ordered_bits(__longlong_as_double(0x7ff0000000000000ll));
+    tissues[t].minmax[1] = ordered_bits(-__longlong_as_double(0x7ff0000000000000ll));
+  }
+}
+
+// ---- set-up kernels ----
+
+// Marks tissue voxels of the full-padded build block with their cell index.
+__global__ void build_voxel_map_kernel(int64_t n, const int64_t* __restrict__ gid, int nx, int ny, int64_t bx,
+                                       int64_t bxy, int64_t* __restrict__ map, int64_t* __restrict__ cellVoxel)
+{
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t g = gid ? gid[i] : i;
+  const int64_t x = g % nx, y = (g / nx) % ny, z = g / ((int64_t)nx * ny);
+  const int64_t v = (x + 1) + bx * (y + 1) + bxy * (z + 1);
+  map[v] = i;
+  cellVoxel[i] = v;
+}
+
+// Weights of every cell (fgr_cell_weights), written in the tissue's class
+// layout: FP64 rows = A0 then the class nodes; mixed rows = class nodes.
+__global__ void build_weights_kernel(int64_t n, const int64_t* __restrict__ map, const int64_t* __restrict__ cellVoxel,
+                                     const double* __restrict__ sigma6, int64_t bx, int64_t bxy, double hx, double hy,
+                                     double hz, int cls, int mixed, void* __restrict__ wout,
+                                     double* __restrict__ w19)
+{
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t v = cellVoxel[i];
+  int tissue[19];
+  int64_t nbrCell[19];
+  for (int k = 0; k < 19; ++k) {
+    const int64_t c = map[v + node_dx(k) + bx * node_dy(k) + bxy * node_dz(k)];
+    nbrCell[k] = c;
+    tissue[k] = c >= 0;
+  }
+  double W[19];
+  fgr_cell_weights(tissue, [&](int k, int c) { return sigma6[6 * nbrCell[k] + c]; }, hx, hy, hz, W);
+  const int rows = class_rows(cls);
+  if (mixed) {
+    float* w = (float*)wout;
+    for (int r = 1; r < rows; ++r) w[(r - 1) * n + i] = (float)W[class_node(cls, r)];
+  } else {
+    double* w = (double*)wout;
+    w[i] = W[0];
+    for (int r = 1; r < rows; ++r) w[r * n + i] = W[class_node(cls, r)];
+  }
+  if (w19)
+    for (int k = 0; k < 19; ++k) w19[k * n + i] = W[k];
+}
+
+// Scatter / gather between cell order and the padded block.
+__global__ void scatter_vm_kernel(int64_t n, const double* __restrict__ src, double* __restrict__ blk,
+                                  const int64_t* __restrict__ voxel, int nx, int ny, int64_t px, int64_t pxy, int py0,
+                                  int pz0)
+{
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int64_t v;
+  if (voxel) v = voxel[i];
+  else {
+    const int64_t x = i % nx, y = (i / nx) % ny, z = i / ((int64_t)nx * ny);
+    v = (x + 1) + px * (y + py0) + pxy * (z + pz0);
+  }
+  blk[v] = src[i];
+}
+
+__global__ void gather_vm_kernel(int64_t n, const double* __restrict__ blk, double* __restrict__ dst,
+                                 const int64_t* __restrict__ voxel, int nx, int ny, int64_t px, int64_t pxy, int py0,
+                                 int pz0)
+{
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int64_t v;
+  if (voxel) v = voxel[i];
+  else {
+    const int64_t x = i % nx, y = (i / nx) % ny, z = i / ((int64_t)nx * ny);
+    v = (x + 1) + px * (y + py0) + pxy * (z + pz0);
+  }
+  dst[i] = blk[v];
+}
+
+__global__ void init_state_kernel(int64_t n, double* s64, float* s32, int mixed, double* act)
+{
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (mixed) {
+    for (int k = 0; k < 5; ++k) s64[k * n + i] = tt06_initial_state(k);
+    for (int k = 5; k < kNumStates; ++k) s32[(k - 5) * n + i] = (float)tt06_initial_state(k);
+  } else {
+    for (int k = 0; k < kNumStates; ++k) s64[k * n + i] = tt06_initial_state(k);
+  }
+  act[i] = -1.0;
+}
+
+__global__ void fill_kernel(int64_t n, double* p, double v)
+{
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+inline unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
+
+// ---- host engine ----
+
+struct DeviceBuffer {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() { release(); }
+  cudaError_t alloc(size_t b)
+  {
+    release();
+    bytes = b;
+    return b ? cudaMalloc(&p, b) : cudaSuccess;
+  }
+  void release()
+  {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  template <typename T>
+  T* as() const { return (T*)p; }
+};
+
+struct HostTissue {
+  TissueDev dev{};
+  std::vector<cdb_stimulus> stims;
+  DeviceBuffer vm0, vm1, s64, s32, w, rtype, voxel, act, minmax;
+  int64_t steps = 0;       // steps taken
+  int parity = 0;
+  int64_t n = 0;
+  int nx = 0, ny = 0, nz = 0;
+};
+
+struct Engine {
+  cdb_engine_config cfg{};
+  cudaStream_t stream = nullptr;
+  int nTypes = 0;
+  std::vector<double> coefPool;   // [type][kFitPoolPerType]
+  TypeTables types{};
+  std::map<int, std::unique_ptr<HostTissue>> tissues;
+  int nextId = 0;
+  bool dirty = true;
+  // tables
+  DeviceBuffer dTissues, dTiles, dStims, dTimes, dStage;
+  std::vector<double> times{0.0};
+  std::vector<int> order;         // tissue ids in table order
+  int64_t nTiles = 0;
+  int64_t launches = 0;
+  // graph of a launch batch
+  cudaGraphExec_t graph = nullptr;
+  int graphSteps = 0;
+  bool graphMinmax = false;
+
+  ~Engine()
+  {
+    if (graph) cudaGraphExecDestroy(graph);
+    tissues.clear();
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  cdb_status ensure_times(int64_t upto)
+  {
+    if ((int64_t)times.size() > upto) {
+      if (dTimes.bytes >= times.size() * sizeof(double)) return CDB_OK;
+    }
+    int64_t want = std::max<int64_t>(upto + 1, (int64_t)times.size() * 2);
+    times.reserve(want);
+    while ((int64_t)times.size() < want) times.push_back(times.back() + cfg.dt);
+    // the reference advances time as time += dt (elec/simulationLoop.cc:230)
+    CDB_CUDA(cudaStreamSynchronize(stream));
+    CDB_CUDA(dTimes.alloc(times.size() * sizeof(double)));
+    CDB_CUDA(cudaMemcpy(dTimes.p, times.data(), times.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    return CDB_OK;
+  }
+
+  cdb_status rebuild()
+  {
+    if (!dirty) return CDB_OK;
+    CDB_CUDA(cudaStreamSynchronize(stream));
+    order.clear();
+    std::vector<TissueDev> devs;
+    std::vector<Tile> tiles;
+    std::vector<cdb_stimulus> stims;
+    for (auto& kv : tissues) {
+      HostTissue& t = *kv.second;
+      t.dev.stim0 = (int)stims.size();
+      t.dev.nstim = (int)t.stims.size();
+      stims.insert(stims.end(), t.stims.begin(), t.stims.end());
+      t.dev.step0 = t.steps;
+      t.dev.parity = t.parity;
+      const int idx = (int)devs.size();
+      devs.push_back(t.dev);
+      order.push_back(kv.first);
+      for (int64_t f = 0; f < t.n; f += kTile) {
+        Tile tl;
+        tl.tissue = idx;
+        tl.first = f;
+        tl.count = (int)std::min<int64_t>(kTile, t.n - f);
+        tiles.push_back(tl);
+      }
+    }
+    nTiles = (int64_t)tiles.size();
+    CDB_CUDA(dTissues.alloc(std::max<size_t>(1, devs.size()) * sizeof(TissueDev)));
+    CDB_CUDA(dTiles.alloc(std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
+    CDB_CUDA(dStims.alloc(std::max<size_t>(1, stims.size()) * sizeof(cdb_stimulus)));
+    if (!devs.empty())
+      CDB_CUDA(cudaMemcpy(dTissues.p, devs.data(), devs.size() * sizeof(TissueDev), cudaMemcpyHostToDevice));
+    if (!tiles.empty())
+      CDB_CUDA(cudaMemcpy(dTiles.p, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+    if (!stims.empty())
+      CDB_CUDA(cudaMemcpy(dStims.p, stims.data(), stims.size() * sizeof(cdb_stimulus), cudaMemcpyHostToDevice));
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    dirty = false;
+    return CDB_OK;
+  }
+
+  // Host copies of step0/parity follow the device ones (advance_kernel).
+  void advance_host(int k)
+  {
+    for (auto& kv : tissues) {
+      kv.second->steps += k;
+      kv.second->parity = (kv.second->parity + k) & 1;
+    }
+  }
+
+  cdb_status launch_batch(int k, bool minmax)
+  {
+    const int nT = (int)order.size();
+    if (minmax) {
+      reset_minmax_kernel<<<grid_for(nT, 128), 128, 0, stream>>>(dTissues.as<TissueDev>(), nT);
+      ++launches;
+    }
+    for (int s = 0; s < k; ++s) {
+      StepArgs a;
+      a.tissues = dTissues.as<TissueDev>();
+      a.tiles = dTiles.as<Tile>();
+      a.stims = dStims.as<cdb_stimulus>();
+      a.times = dTimes.as<double>();
+      a.dt = cfg.dt;
+      a.k = s;
+      a.minmax = (minmax && s == k - 1) ? 1 : 0;
+      if (cfg.precision == CDB_MIXED)
+        fused_step_kernel<true><<<(unsigned)nTiles, kTile, 0, stream>>>(a);
+      else
+        fused_step_kernel<false><<<(unsigned)nTiles, kTile, 0, stream>>>(a);
+      ++launches;
+    }
+    advance_kernel<<<grid_for(nT, 128), 128, 0, stream>>>(dTissues.as<TissueDev>(), nT, k);
+    ++launches;
+    return CDB_OK;
+  }
+
+  cdb_status step(int k, bool minmax = true)
+  {
+    CDB_CHECK(k >= 0, CDB_INVALID_ARG, "nSteps must be >= 0");
+    if (k == 0 || tissues.empty()) return CDB_OK;
+    cdb_status st = rebuild();
+    if (st != CDB_OK) return st;
+    int64_t maxStep = 0;
+    for (auto& kv : tissues) maxStep = std::max(maxStep, kv.second->steps);
+    st = ensure_times(maxStep + k + 1);
+    if (st != CDB_OK) return st;
+    if (cfg.use_graphs) {
+      if (!graph || graphSteps != k || graphMinmax != minmax) {
+        if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+        cudaGraph_t g;
+        CDB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        const int64_t before = launches;
+        launch_batch(k, minmax);
+        const int64_t perBatch = launches - before;
+        launches = before;
+        CDB_CUDA(cudaStreamEndCapture(stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        CDB_CUDA(e);
+        graphSteps = k;
+        graphMinmax = minmax;
+        graphLaunches = perBatch;
+      }
+      CDB_CUDA(cudaGraphLaunch(graph, stream));
+      launches += graphLaunches;
+    } else {
+      launch_batch(k, minmax);
+    }
+    CDB_CUDA(cudaGetLastError());
+    advance_host(k);
+    return CDB_OK;
+  }
+  int64_t graphLaunches = 0;
+};
+
+}  // namespace cdb
+
+using namespace cdb;
+
+struct cdb_engine {
+  Engine e;
+};
+
+namespace {
+
+HostTissue* find_tissue(cdb_engine* e, int32_t id)
+{
+  auto it = e->e.tissues.find(id);
+  return it == e->e.tissues.end() ? nullptr : it->second.get();
+}
+
+int tissue_class(int nx, int ny, int nz, bool masked)
+{
+  if (masked) return kVolume;
+  if (ny == 1 && nz == 1) return kCable;
+  if (nz == 1) return kSheet;
+  return kVolume;
+}
+
+cdb_status validate_desc(const Engine& E, const cdb_tissue_desc* t)
+{
+  CDB_CHECK(t, CDB_INVALID_ARG, "null tissue descriptor");
+  CDB_CHECK(t->nx > 0 && t->ny > 0 && t->nz > 0, CDB_INVALID_ARG, "grid dimensions must be positive");
+  CDB_CHECK(t->dx > 0 && t->dy > 0 && t->dz > 0, CDB_INVALID_ARG, "grid spacing must be positive");
+  const int64_t grid = (int64_t)t->nx * t->ny * t->nz;
+  CDB_CHECK(t->nCells > 0 && t->nCells <= grid, CDB_INVALID_ARG, "nCells must be in [1, nx*ny*nz]");
+  CDB_CHECK(t->nCells < (int64_t(1) << 31), CDB_INVALID_ARG, "a tissue holds fewer than 2^31 cells");
+  CDB_CHECK(t->gid || t->nCells == grid, CDB_INVALID_ARG, "gid may be NULL only for a full grid");
+  CDB_CHECK(t->cellType && t->reaction && t->sigma6, CDB_INVALID_ARG, "cellType, reaction and sigma6 are required");
+  CDB_CHECK(t->nStim >= 0 && t->nStim <= CDB_MAX_STIM_PER_TISSUE, CDB_INVALID_ARG, "too many stimuli for one tissue");
+  CDB_CHECK(t->nStim == 0 || t->stim, CDB_INVALID_ARG, "stim is NULL");
+  for (int64_t i = 0; i < t->nCells; ++i) {
+    CDB_CHECK(t->cellType[i] > 0, CDB_INVALID_ARG, "cellType must be > 0 (tissue) for every cell");
+    CDB_CHECK(t->reaction[i] < E.nTypes, CDB_INVALID_ARG, "reaction id out of range");
+    if (t->gid) {
+      CDB_CHECK(t->gid[i] >= 0 && t->gid[i] < grid, CDB_INVALID_ARG, "gid outside the grid");
+      CDB_CHECK(i == 0 || t->gid[i] > t->gid[i - 1], CDB_INVALID_ARG, "gids must be strictly increasing");
+    }
+  }
+  for (int s = 0; s < t->nStim; ++s)
+    CDB_CHECK(t->stim[s].period > 0 && t->stim[s].duration > 0, CDB_INVALID_ARG, "stimulus period and duration must be > 0");
+  return CDB_OK;
+}
+
+int64_t padded_voxels(int nx, int ny, int nz, int cls, int64_t* px, int64_t* pxy, int* py0, int* pz0)
+{
+  const int64_t Px = nx + 2;
+  const int64_t Py = cls >= kSheet ? ny + 2 : 1;
+  const int64_t Pz = cls == kVolume ? nz + 2 : 1;
+  if (px) *px = Px;
+  if (pxy) *pxy = Px * Py;
+  if (py0) *py0 = cls >= kSheet ? 1 : 0;
+  if (pz0) *pz0 = cls == kVolume ? 1 : 0;
+  return Px * Py * Pz;
+}
+
+int64_t tissue_bytes(const Engine& E, const cdb_tissue_desc* t)
+{
+  const bool masked = t->gid && t->nCells != (int64_t)t->nx * t->ny * t->nz;
+  const int cls = tissue_class(t->nx, t->ny, t->nz, masked);
+  const int64_t vox = padded_voxels(t->nx, t->ny, t->nz, cls, nullptr, nullptr, nullptr, nullptr);
+  const int64_t n = t->nCells;
+  const bool mixed = E.cfg.precision == CDB_MIXED;
+  int64_t b = 2 * vox * 8;                                   // Vm blocks
+  b += mixed ? n * (5 * 8 + 13 * 4) : n * 18 * 8;           // state
+  b += mixed ? n * (class_rows(cls) - 1) * 4 : n * class_rows(cls) * 8;   // weights
+  b += n + n * 8 + (masked ? n * 8 : 0) + 64;               // rtype, act, voxel
+  return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cdb_last_error(void) { return t_last_error.c_str(); }
+const char* cdb_version(void) { return "cardioid_b200 0.1 (sm_100a)"; }
+
+double cdb_fit_eval(const cdb_fit* f, double x)
+{
+  const double* c = f->coeff;
+  double num = c[f->numer - 1];
+  for (int k = f->numer - 2; k >= 0; --k) num = c[k] + x * num;
+  if (f->denom == 1) return num;
+  const double* d = c + f->numer;
+  double den = d[f->denom - 2];
+  for (int k = f->denom - 3; k >= 0; --k) den = d[k] + x * den;
+  den = 1 + x * den;
+  return num / den;
+}
+
+cdb_status cdb_engine_create(const cdb_engine_config* cfg, cdb_engine** out)
+{
+  CDB_CHECK(cfg && out, CDB_INVALID_ARG, "null argument");
+  CDB_CHECK(cfg->dt > 0, CDB_INVALID_ARG, "dt must be > 0");
+  CDB_CHECK(cfg->precision == CDB_FP64 || cfg->precision == CDB_MIXED, CDB_INVALID_ARG, "unknown precision");
+  int nDev = 0;
+  CDB_CUDA(cudaGetDeviceCount(&nDev));
+  CDB_CHECK(cfg->device >= 0 && cfg->device < nDev, CDB_INVALID_ARG, "no such device");
+  CDB_CUDA(cudaSetDevice(cfg->device));
+  std::unique_ptr<cdb_engine> e(new cdb_engine);
+  e->e.cfg = *cfg;
+  CDB_CUDA(cudaStreamCreateWithFlags(&e->e.stream, cudaStreamNonBlocking));
+  e->e.coefPool.assign((size_t)CDB_MAX_REACTION_TYPES * kFitPoolPerType, 0.0);
+  *out = e.release();
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_destroy(cdb_engine* e)
+{
+  if (!e) return CDB_OK;
+  cudaSetDevice(e->e.cfg.device);
+  cudaStreamSynchronize(e->e.stream);
+  delete e;
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_add_reaction(cdb_engine* e, const cdb_tt06_params* params, const cdb_fit fits[CDB_NUM_FITS],
+                                   int32_t* id)
+{
+  CDB_CHECK(e && params && fits && id, CDB_INVALID_ARG, "null argument");
+  Engine& E = e->e;
+  CDB_CHECK(E.nTypes < CDB_MAX_REACTION_TYPES, CDB_INVALID_ARG, "too many reaction types");
+  const int t = E.nTypes;
+  std::string err;
+  double* pool = E.coefPool.data() + (size_t)t * kFitPoolPerType;
+  CDB_CHECK(pack_fits(fits, E.types.shape[t], pool, kFitPoolPerType, err), CDB_INVALID_ARG, err);
+  E.types.scal[t] = to_scalars(*params);
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  std::vector<float> pool32(E.coefPool.size());
+  for (size_t k = 0; k < pool32.size(); ++k) pool32[k] = (float)E.coefPool[k];
+  CDB_CUDA(cudaMemcpyToSymbol(c_scal, E.types.scal, sizeof(E.types.scal)));
+  CDB_CUDA(cudaMemcpyToSymbol(c_shape, E.types.shape, sizeof(E.types.shape)));
+  CDB_CUDA(cudaMemcpyToSymbol(c_coef64, E.coefPool.data(), E.coefPool.size() * sizeof(double)));
+  CDB_CUDA(cudaMemcpyToSymbol(c_coef32, pool32.data(), pool32.size() * sizeof(float)));
+  E.nTypes = t + 1;
+  *id = t;
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_tissue_bytes(cdb_engine* e, const cdb_tissue_desc* t, int64_t* bytes)
+{
+  CDB_CHECK(e && t && bytes, CDB_INVALID_ARG, "null argument");
+  *bytes = tissue_bytes(e->e, t);
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_free_bytes(cdb_engine* e, int64_t* freeBytes, int64_t* totalBytes)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  CDB_CUDA(cudaSetDevice(e->e.cfg.device));
+  size_t f = 0, t = 0;
+  CDB_CUDA(cudaMemGetInfo(&f, &t));
+  if (freeBytes) *freeBytes = (int64_t)f;
+  if (totalBytes) *totalBytes = (int64_t)t;
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_t* id)
+{
+  CDB_CHECK(e && id, CDB_INVALID_ARG, "null argument");
+  Engine& E = e->e;
+  cdb_status st = validate_desc(E, t);
+  if (st != CDB_OK) return st;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  const bool mixed = E.cfg.precision == CDB_MIXED;
+  const int64_t n = t->nCells;
+  const int64_t gridN = (int64_t)t->nx * t->ny * t->nz;
+  const bool masked = t->gid && n != gridN;
+  const int cls = tissue_class(t->nx, t->ny, t->nz, masked);
+  std::unique_ptr<HostTissue> h(new HostTissue);
+  h->n = n;
+  h->nx = t->nx; h->ny = t->ny; h->nz = t->nz;
+  TissueDev& d = h->dev;
+  d.n = n;
+  d.nx = t->nx; d.ny = t->ny; d.nz = t->nz;
+  d.cls = cls;
+  const int64_t vox = padded_voxels(t->nx, t->ny, t->nz, cls, &d.px, &d.pxy, &d.py0, &d.pz0);
+  d.scale = t->diffusionScale;
+  d.blk.g_Kr = t->g_Kr_scale; d.blk.g_CaL = t->g_CaL_scale; d.blk.g_Na = t->g_Na_scale;
+  h->stims.assign(t->stim, t->stim + t->nStim);
+
+  cudaStream_t s = E.stream;
+  CDB_CUDA(cudaStreamSynchronize(s));
+  CDB_CUDA(h->vm0.alloc(vox * 8));
+  CDB_CUDA(h->vm1.alloc(vox * 8));
+  CDB_CUDA(cudaMemsetAsync(h->vm0.p, 0, vox * 8, s));
+  CDB_CUDA(cudaMemsetAsync(h->vm1.p, 0, vox * 8, s));
+  if (mixed) {
+    CDB_CUDA(h->s64.alloc(n * 5 * 8));
+    CDB_CUDA(h->s32.alloc(n * 13 * 4));
+  } else {
+    CDB_CUDA(h->s64.alloc(n * 18 * 8));
+  }
+  const int rows = class_rows(cls);
+  CDB_CUDA(h->w.alloc(mixed ? n * (rows - 1) * 4 : n * rows * 8));
+  CDB_CUDA(h->rtype.alloc(n));
+  CDB_CUDA(h->act.alloc(n * 8));
+  CDB_CUDA(h->minmax.alloc(16));
+  if (masked) CDB_CUDA(h->voxel.alloc(n * 8));
+
+  // set-up scratch: full-padded voxel map, cell voxels, sigma, gids
+  {
+    const int64_t bx = t->nx + 2, bxy = bx * (t->ny + 2);
+    const int64_t bvox = bxy * (t->nz + 2);
+    DeviceBuffer map, cellVoxel, sig, gid, host64;
+    CDB_CUDA(map.alloc(bvox * 8));
+    CDB_CUDA(cellVoxel.alloc(n * 8));
+    CDB_CUDA(sig.alloc(n * 6 * 8));
+    if (t->gid) {
+      CDB_CUDA(gid.alloc(n * 8));
+      CDB_CUDA(cudaMemcpyAsync(gid.p, t->gid, n * 8, cudaMemcpyHostToDevice, s));
+    }
+    CDB_CUDA(cudaMemsetAsync(map.p, 0xff, bvox * 8, s));   // -1: no cell
+    CDB_CUDA(cudaMemcpyAsync(sig.p, t->sigma6, n * 6 * 8, cudaMemcpyHostToDevice, s));
+    build_voxel_map_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, gid.as<int64_t>(), t->nx, t->ny, bx, bxy,
+                                                            map.as<int64_t>(), cellVoxel.as<int64_t>());
+    build_weights_kernel<<<grid_for(n, 128), 128, 0, s>>>(n, map.as<int64_t>(), cellVoxel.as<int64_t>(),
+                                                          sig.as<double>(), bx, bxy, t->dx, t->dy, t->dz, cls,
+                                                          mixed ? 1 : 0, h->w.p, nullptr);
+    E.launches += 2;
+    if (masked) {
+      // cell voxels in the engine's (class-padded) block; masked tissues are kVolume
+      std::vector<int64_t> v(n);
+      const int64_t Px = d.px, Pxy = d.pxy;
+      for (int64_t i = 0; i < n; ++i) {
+        const int64_t g = t->gid[i];
+        const int64_t x = g % t->nx, y = (g / t->nx) % t->ny, z = g / ((int64_t)t->nx * t->ny);
+        v[i] = (x + 1) + Px * (y + d.py0) + Pxy * (z + d.pz0);
+      }
+      CDB_CUDA(cudaMemcpyAsync(h->voxel.p, v.data(), n * 8, cudaMemcpyHostToDevice, s));
+      CDB_CUDA(cudaStreamSynchronize(s));
+    }
+    CDB_CUDA(cudaMemcpyAsync(h->rtype.p, t->reaction, n, cudaMemcpyHostToDevice, s));
+    CDB_CUDA(cudaStreamSynchronize(s));
+  }
+  d.vm[0] = h->vm0.as<double>();
+  d.vm[1] = h->vm1.as<double>();
+  d.s64 = h->s64.as<double>();
+  d.s32 = h->s32.as<float>();
+  d.w = h->w.p;
+  d.rtype = h->rtype.as<uint8_t>();
+  d.voxel = masked ? h->voxel.as<int64_t>() : nullptr;
+  d.act = h->act.as<double>();
+  d.minmax = h->minmax.as<unsigned long long>();
+  init_state_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, d.s64, d.s32, mixed ? 1 : 0, d.act);
+  E.launches += 1;
+  {
+    DeviceBuffer v0;
+    CDB_CUDA(v0.alloc(n * 8));
+    if (t->vm0) {
+      CDB_CUDA(cudaMemcpyAsync(v0.p, t->vm0, n * 8, cudaMemcpyHostToDevice, s));
+    } else {
+      fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, v0.as<double>(), kInitialVm);
+      E.launches += 1;
+    }
+    scatter_vm_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, v0.as<double>(), d.vm[0], d.voxel, d.nx, d.ny, d.px,
+                                                       d.pxy, d.py0, d.pz0);
+    E.launches += 1;
+    CDB_CUDA(cudaStreamSynchronize(s));
+  }
+  CDB_CUDA(cudaGetLastError());
+  const int newId = E.nextId++;
+  E.tissues[newId] = std::move(h);
+  E.dirty = true;
+  *id = newId;
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_remove_tissue(cdb_engine* e, int32_t id)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  Engine& E = e->e;
+  auto it = E.tissues.find(id);
+  CDB_CHECK(it != E.tissues.end(), CDB_NOT_FOUND, "no tissue with that id");
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  E.tissues.erase(it);
+  E.dirty = true;
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_step(cdb_engine* e, int32_t nSteps)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  CDB_CUDA(cudaSetDevice(e->e.cfg.device));
+  return e->e.step(nSteps, true);
+}
+
+cdb_status cdb_engine_sync(cdb_engine* e)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  CDB_CUDA(cudaSetDevice(e->e.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(e->e.stream));
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_tissue_time(cdb_engine* e, int32_t id, int64_t* steps, double* time)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  Engine& E = e->e;
+  cdb_status st = E.ensure_times(t->steps + 1);
+  if (st != CDB_OK) return st;
+  if (steps) *steps = t->steps;
+  if (time) *time = E.times[t->steps];
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_read_vm(cdb_engine* e, int32_t id, double* host)
+{
+  CDB_CHECK(e && host, CDB_INVALID_ARG, "null argument");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  Engine& E = e->e;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  DeviceBuffer tmp;
+  CDB_CUDA(tmp.alloc(t->n * 8));
+  const TissueDev& d = t->dev;
+  gather_vm_kernel<<<grid_for(t->n, 256), 256, 0, E.stream>>>(t->n, d.vm[t->parity], tmp.as<double>(), d.voxel,
+                                                             d.nx, d.ny, d.px, d.pxy, d.py0, d.pz0);
+  E.launches += 1;
+  CDB_CUDA(cudaMemcpyAsync(host, tmp.p, t->n * 8, cudaMemcpyDeviceToHost, E.stream));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_write_vm(cdb_engine* e, int32_t id, const double* host)
+{
+  CDB_CHECK(e && host, CDB_INVALID_ARG, "null argument");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  Engine& E = e->e;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  DeviceBuffer tmp;
+  CDB_CUDA(tmp.alloc(t->n * 8));
+  CDB_CUDA(cudaMemcpyAsync(tmp.p, host, t->n * 8, cudaMemcpyHostToDevice, E.stream));
+  const TissueDev& d = t->dev;
+  scatter_vm_kernel<<<grid_for(t->n, 256), 256, 0, E.stream>>>(t->n, tmp.as<double>(), d.vm[t->parity], d.voxel,
+                                                              d.nx, d.ny, d.px, d.pxy, d.py0, d.pz0);
+  E.launches += 1;
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_read_state(cdb_engine* e, int32_t id, int var, double* host)
+{
+  CDB_CHECK(e && host, CDB_INVALID_ARG, "null argument");
+  CDB_CHECK(var >= 0 && var < kNumStates, CDB_INVALID_ARG, "state index out of range");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  Engine& E = e->e;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  const int64_t n = t->n;
+  if (E.cfg.precision == CDB_MIXED && var >= 5) {
+    std::vector<float> tmp(n);
+    CDB_CUDA(cudaMemcpy(tmp.data(), t->dev.s32 + (var - 5) * n, n * 4, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < n; ++i) host[i] = tmp[i];
+  } else {
+    CDB_CUDA(cudaMemcpy(host, t->dev.s64 + var * n, n * 8, cudaMemcpyDeviceToHost));
+  }
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_write_state(cdb_engine* e, int32_t id, int var, const double* host)
+{
+  CDB_CHECK(e && host, CDB_INVALID_ARG, "null argument");
+  CDB_CHECK(var >= 0 && var < kNumStates, CDB_INVALID_ARG, "state index out of range");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  Engine& E = e->e;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  const int64_t n = t->n;
+  if (E.cfg.precision == CDB_MIXED && var >= 5) {
+    std::vector<float> tmp(n);
+    for (int64_t i = 0; i < n; ++i) tmp[i] = (float)host[i];
+    CDB_CUDA(cudaMemcpy(t->dev.s32 + (var - 5) * n, tmp.data(), n * 4, cudaMemcpyHostToDevice));
+  } else {
+    CDB_CUDA(cudaMemcpy(t->dev.s64 + var * n, host, n * 8, cudaMemcpyHostToDevice));
+  }
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_read_activation(cdb_engine* e, int32_t id, double* host)
+{
+  CDB_CHECK(e && host, CDB_INVALID_ARG, "null argument");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  Engine& E = e->e;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  CDB_CUDA(cudaMemcpy(host, t->dev.act, t->n * 8, cudaMemcpyDeviceToHost));
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_minmax(cdb_engine* e, int32_t id, double* vmin, double* vmax)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  Engine& E = e->e;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  unsigned long long mm[2];
+  CDB_CUDA(cudaMemcpy(mm, t->dev.minmax, 16, cudaMemcpyDeviceToHost));
+  if (vmin) *vmin = from_ordered_bits(mm[0]);
+  if (vmax) *vmax = from_ordered_bits(mm[1]);
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_read_weights(cdb_engine* e, int32_t id, double* host19)
+{
+  CDB_CHECK(e && host19, CDB_INVALID_ARG, "null argument");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  Engine& E = e->e;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  const int64_t n = t->n;
+  const int cls = t->dev.cls;
+  const int rows = class_rows(cls);
+  const bool mixed = E.cfg.precision == CDB_MIXED;
+  std::vector<double> out(n * 19, 0.0);
+  if (mixed) {
+    std::vector<float> w((size_t)n * (rows - 1));
+    CDB_CUDA(cudaMemcpy(w.data(), t->dev.w, w.size() * 4, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < n; ++i) {
+      double a0 = 0;
+      for (int r = 1; r < rows; ++r) {
+        out[i * 19 + class_node(cls, r)] = w[(r - 1) * n + i];
+        a0 -= w[(r - 1) * n + i];
+      }
+      out[i * 19] = a0;
+    }
+  } else {
+    std::vector<double> w((size_t)n * rows);
+    CDB_CUDA(cudaMemcpy(w.data(), t->dev.w, w.size() * 8, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < n; ++i)
+      for (int r = 0; r < rows; ++r) out[i * 19 + class_node(cls, r)] = w[r * n + i];
+  }
+  std::memcpy(host19, out.data(), out.size() * 8);
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, double* vm_out)
+{
+  CDB_CHECK(e && vm_in && vm_out, CDB_INVALID_ARG, "null argument");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  Engine& E = e->e;
+  CDB_CHECK(E.tissues.size() == 1, CDB_INVALID_ARG, "cdb_engine_step_host needs an engine with one tissue");
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  const int64_t n = t->n;
+  if (E.dStage.bytes < (size_t)n * 8) CDB_CUDA(E.dStage.alloc(n * 8));
+  const TissueDev& d = t->dev;
+  cudaStream_t s = E.stream;
+  CDB_CUDA(cudaMemcpyAsync(E.dStage.p, vm_in, n * 8, cudaMemcpyHostToDevice, s));
+  scatter_vm_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, E.dStage.as<double>(), d.vm[t->parity], d.voxel, d.nx, d.ny,
+                                                     d.px, d.pxy, d.py0, d.pz0);
+  E.launches += 1;
+  cdb_status st = E.step(1, false);
+  if (st != CDB_OK) return st;
+  gather_vm_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, d.vm[t->parity], E.dStage.as<double>(), d.voxel, d.nx, d.ny,
+                                                    d.px, d.pxy, d.py0, d.pz0);
+  E.launches += 1;
+  CDB_CUDA(cudaMemcpyAsync(vm_out, E.dStage.p, n * 8, cudaMemcpyDeviceToHost, s));
+  CDB_CUDA(cudaStreamSynchronize(s));
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_launch_count(cdb_engine* e, int64_t* launches)
+{
+  CDB_CHECK(e && launches, CDB_INVALID_ARG, "null argument");
+  *launches = e->e.launches;
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_stream(cdb_engine* e, void** stream)
+{
+  CDB_CHECK(e && stream, CDB_INVALID_ARG, "null argument");
+  *stream = (void*)e->e.stream;
+  return CDB_OK;
+}
+
+}  // extern "C"

@@ -115,11 +115,7 @@ def params_from_object(db, name, dt, generate=None):
         fgk1 = objectdb.get_float(fobj, "g_K1", float("nan"))
         funcs = objectdb.get_list(fobj, "functions")
         if fdt == dt and fct == p.celltype and fgk1 == p.g_K1 and len(funcs) == NFIT:
-            fits = []
-            for fn in funcs:
-                f = db.find(fn, "FUNCTION")
-                fits.append(Fit(int(objectdb.get_float(f, "numer", -1)), int(objectdb.get_float(f, "denom", -1)),
-                                objectdb.get_floats(f, "coeff")))
+            fits = fits_from_fit_object(db, fit_name)
     if fits is None:
         if generate is None:
             raise ValueError("REACTION %s: no reusable FIT for dt=%g celltype=%g g_K1=%g" % (name, dt, p.celltype, p.g_K1))
@@ -129,6 +125,18 @@ def params_from_object(db, name, dt, generate=None):
             raise ValueError("REACTION %s: malformed fit (numer=%d denom=%d, %d coeffs)" % (name, f.numer, f.denom, len(f.coeff)))
     p.fits = fits
     return p
+
+
+def fits_from_fit_object(db, fit_name):
+    """The 30 Fits listed by a FIT object, read from its FUNCTION objects
+    (keys numer, denom, coeff; elec/BetterTT06.cc:140-147)."""
+    fobj = db.find(fit_name, "FIT")
+    fits = []
+    for fn in objectdb.get_list(fobj, "functions"):
+        f = db.find(fn, "FUNCTION")
+        fits.append(Fit(int(objectdb.get_float(f, "numer", -1)), int(objectdb.get_float(f, "denom", -1)),
+                        objectdb.get_floats(f, "coeff")))
+    return fits
 
 
 def fit_file_text(reaction_name, dt, params):

@@ -1,0 +1,203 @@
+/*
+ * cardioid_b200 — C ABI of the B200 engine for Cardioid's monodomain hot path.
+ *
+ * Plain pointers and sizes only; every call returns a cdb_status and never
+ * throws or aborts.  cdb_last_error() gives the message of the calling
+ * thread's last failure.  Pointers documented as "device" are CUDA device
+ * pointers on the engine's device; all others are host pointers.
+ *
+ * Three groups of entry points, each standing in for one reference
+ * interface (paths are relative to the LLNL/Cardioid checkout):
+ *
+ *   cdb_reaction_*  — the Reaction plugin (elec/Reaction.hh:10-40) for
+ *                     BetterTT06 (elec/BetterTT06.hh, elec/BetterTT06.cc).
+ *   cdb_fgr_*       — the Diffusion plugin (elec/Diffusion.hh:19-39) for the
+ *                     FGR stencil (elec/FGRDiffusionOMP.hh/.cc).
+ *   cdb_engine_*    — the omp time loop (elec/simulationLoop.cc:150-243) with
+ *                     reaction, diffusion, box stimuli, integrator and the
+ *                     activation/min-max sensors fused into one kernel per
+ *                     step, over one or many tissues.
+ */
+#ifndef CARDIOID_B200_H
+#define CARDIOID_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CDB_OK = 0,
+  CDB_INVALID_ARG = 1,   /* a size, index, key or pointer the call cannot accept */
+  CDB_OOM = 2,           /* device memory could not be allocated */
+  CDB_CUDA_ERROR = 3,    /* a CUDA runtime call or kernel launch failed */
+  CDB_NUMERIC_FAULT = 4, /* a non-finite Vm was detected */
+  CDB_TIMEOUT = 5,       /* a bounded device wait gave up */
+  CDB_NOT_FOUND = 6      /* no tissue or reaction with that id */
+} cdb_status;
+
+typedef enum { CDB_FP64 = 0, CDB_MIXED = 1 } cdb_precision;
+
+#define CDB_NUM_FITS 30
+#define CDB_NUM_STATES 18
+#define CDB_MAX_COEFF 64
+#define CDB_MAX_REACTION_TYPES 6
+#define CDB_MAX_STIM_PER_TISSUE 32
+
+/* One rational fit in the reference's FUNCTION-object form
+ * (elec/Interpolation.hh:11-99): numer numerator coefficients then denom-1
+ * denominator coefficients, monomial, denominator constant 1. */
+typedef struct {
+  int32_t numer;
+  int32_t denom;
+  double coeff[CDB_MAX_COEFF];
+} cdb_fit;
+
+/* Scalar parameters of one BetterTT06 REACTION object
+ * (reactionFactoryForBetterTT06, elec/BetterTT06.cc:69-121). */
+typedef struct {
+  double celltype, g_CaL, g_K1, g_Kr, g_Ks, g_Na, g_bca, g_bna, g_pCa, g_pK, g_to;
+} cdb_tt06_params;
+
+/* A BoxStimulus with a PeriodicPulse (elec/BoxStimulus.cc:11-70,
+ * elec/PeriodicPulse.cc:22-28, elec/Stimulus.hh:21-27): while
+ * t0 < time < tf and phase <= time mod period < phase + duration, cells with
+ * xMin < x < xMax, yMin < y < yMax, zMin < z < zMax get iStim = amplitude
+ * (= -vStim); a later stimulus overwrites an earlier one. */
+typedef struct {
+  double t0, tf, period, duration, amplitude, phase;
+  double xMin, xMax, yMin, yMax, zMin, zMax;
+} cdb_stimulus;
+
+/* ------------------------------------------------------------------ */
+/* Library                                                              */
+/* ------------------------------------------------------------------ */
+const char* cdb_last_error(void);
+const char* cdb_version(void);
+/* Evaluates one fit on the host (Interpolation::eval). */
+double cdb_fit_eval(const cdb_fit* fit, double x);
+
+/* ------------------------------------------------------------------ */
+/* Reaction plugin: BetterTT06 on the device.                           */
+/* Replaces BetterTT06::ThisReaction (elec/BetterTT06.hh:49-112):       */
+/*   constructor + reactionFactoryForBetterTT06   -> cdb_reaction_create */
+/*   initializeMembraneVoltage (BetterTT06.cc:1657) -> cdb_reaction_init */
+/*   calc (Reaction.hh:15-19, BetterTT06.cc:1320)   -> cdb_reaction_calc */
+/*   getValue / setValue (BetterTT06.cc:1860-2210)  -> cdb_reaction_{get,set}_state */
+/* ------------------------------------------------------------------ */
+typedef struct cdb_reaction cdb_reaction;
+
+cdb_status cdb_reaction_create(int device, cdb_precision precision, const cdb_tt06_params* params,
+                               const cdb_fit fits[CDB_NUM_FITS], int64_t nCells, double dt,
+                               cdb_reaction** out);
+/* indexArray (device, int32[nCells]) lists this reaction's cells in the
+ * caller's Vm array; Vm (device) gets V_init at those positions. */
+cdb_status cdb_reaction_init(cdb_reaction* r, const int32_t* indexArray, double* Vm, void* stream);
+/* dVm[indexArray[i]] = -Iion(Vm[indexArray[i]], state_i); state advanced
+ * by dt.  iStim is accepted and unused, as in the reference.  All device
+ * pointers; stream is a cudaStream_t (NULL = default stream). */
+cdb_status cdb_reaction_calc(cdb_reaction* r, double dt, const int32_t* indexArray, const double* Vm,
+                             const double* iStim, double* dVm, void* stream);
+/* var in checkpoint order (Ca_SR Ca_i Ca_ss K_i Na_i R_prime Xr1 Xr2 Xs d f
+ * f2 fCass h j m r s); host arrays of nCells doubles. */
+cdb_status cdb_reaction_get_state(cdb_reaction* r, int var, double* host);
+cdb_status cdb_reaction_set_state(cdb_reaction* r, int var, const double* host);
+cdb_status cdb_reaction_destroy(cdb_reaction* r);
+
+/* ------------------------------------------------------------------ */
+/* Diffusion plugin: FGR 19-point stencil on the device.                */
+/* Replaces FGRDiffusionOMP (elec/FGRDiffusionOMP.hh:13-44):            */
+/*   constructor + precomputeCoefficients    -> cdb_fgr_create          */
+/*   updateLocalVoltage (FGRDiffusionOMP.cc:75) -> cdb_fgr_update_local_voltage */
+/*   calc (FGRDiffusionOMP.cc:109, assigns dVm) -> cdb_fgr_calc         */
+/* ------------------------------------------------------------------ */
+typedef struct cdb_fgr cdb_fgr;
+
+/* Cells (host arrays) in local order: gid = x + nx*(y + ny*z) on the
+ * nx*ny*nz grid, anatomy cellType (> 0 is tissue) and the conductivity
+ * tensor as a11 a12 a13 a22 a23 a33 (S/mm); spacing in mm;
+ * diffusionScale in mm^3/mF. */
+cdb_status cdb_fgr_create(int device, int32_t nx, int32_t ny, int32_t nz, double dx, double dy, double dz,
+                          int64_t nCells, const int64_t* gid, const int32_t* cellType, const double* sigma6,
+                          double diffusionScale, cdb_fgr** out);
+cdb_status cdb_fgr_update_local_voltage(cdb_fgr* d, const double* Vm, void* stream);
+cdb_status cdb_fgr_calc(cdb_fgr* d, double* dVm, void* stream);
+/* The weights the stencil uses (host, nCells x 19: A0 then A[1..18] in the
+ * reference's NodeLocation order). */
+cdb_status cdb_fgr_get_weights(cdb_fgr* d, double* host19);
+cdb_status cdb_fgr_destroy(cdb_fgr* d);
+
+/* ------------------------------------------------------------------ */
+/* Fused engine                                                          */
+/* ------------------------------------------------------------------ */
+typedef struct cdb_engine cdb_engine;
+
+typedef struct {
+  int device;
+  cdb_precision precision;
+  double dt;               /* ms */
+  int use_graphs;          /* capture step batches as CUDA graphs */
+} cdb_engine_config;
+
+typedef struct {
+  int32_t nx, ny, nz;          /* grid; gid = x + nx*(y + ny*z) */
+  double dx, dy, dz;           /* mm */
+  int64_t nCells;
+  const int64_t* gid;          /* NULL: all nx*ny*nz cells in gid order */
+  const int32_t* cellType;     /* anatomy cellType per cell, > 0 */
+  const uint8_t* reaction;     /* reaction-type id per cell */
+  const double* sigma6;        /* nCells x 6 */
+  const double* vm0;           /* initial Vm per cell; NULL: V_init */
+  double diffusionScale;       /* mm^3/mF; 0 disables diffusion */
+  float g_Kr_scale, g_CaL_scale, g_Na_scale;   /* drug block multipliers (1 = none) */
+  int32_t nStim;
+  const cdb_stimulus* stim;
+} cdb_tissue_desc;
+
+cdb_status cdb_engine_create(const cdb_engine_config* cfg, cdb_engine** out);
+cdb_status cdb_engine_destroy(cdb_engine* e);
+/* Registers a BetterTT06 parameter set; *id is used in cdb_tissue_desc.reaction. */
+cdb_status cdb_engine_add_reaction(cdb_engine* e, const cdb_tt06_params* params,
+                                   const cdb_fit fits[CDB_NUM_FITS], int32_t* id);
+/* Device bytes a tissue would take (for admission by free memory). */
+cdb_status cdb_engine_tissue_bytes(cdb_engine* e, const cdb_tissue_desc* t, int64_t* bytes);
+cdb_status cdb_engine_free_bytes(cdb_engine* e, int64_t* free_bytes, int64_t* total_bytes);
+/* Adds a tissue between steps; its time starts at 0. */
+cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_t* id);
+cdb_status cdb_engine_remove_tissue(cdb_engine* e, int32_t id);
+/* Advances every tissue by nSteps steps of dt (one fused kernel per step). */
+cdb_status cdb_engine_step(cdb_engine* e, int32_t nSteps);
+/* Blocks until the engine's stream is idle. */
+cdb_status cdb_engine_sync(cdb_engine* e);
+/* Number of steps a tissue has taken and its time (ms, accumulated as
+ * time += dt like the reference). */
+cdb_status cdb_engine_tissue_time(cdb_engine* e, int32_t id, int64_t* steps, double* time);
+/* Host copies, cell order of the tissue. */
+cdb_status cdb_engine_read_vm(cdb_engine* e, int32_t id, double* host);
+cdb_status cdb_engine_write_vm(cdb_engine* e, int32_t id, const double* host);
+cdb_status cdb_engine_read_state(cdb_engine* e, int32_t id, int var, double* host);
+cdb_status cdb_engine_write_state(cdb_engine* e, int32_t id, int var, const double* host);
+/* First post-step time with Vm > 0 per cell, -1 if never
+ * (ActivationTimeSensor::eval, elec/ActivationTimeSensor.cc:99-111). */
+cdb_status cdb_engine_read_activation(cdb_engine* e, int32_t id, double* host);
+/* min/max Vm of a tissue after the last step (MinMaxSensor, elec/MinMaxSensor.cc:44-67). */
+cdb_status cdb_engine_minmax(cdb_engine* e, int32_t id, double* vmin, double* vmax);
+/* Weights of a tissue (host, nCells x 19, A0 then A[1..18]), as built. */
+cdb_status cdb_engine_read_weights(cdb_engine* e, int32_t id, double* host19);
+/* One step through host buffers: copies vm_in (host) to the device, takes
+ * one fused step of the tissue and copies the new Vm to vm_out (host).
+ * The reaction state stays on the device, as a Reaction object keeps its
+ * own state; this is the per-step cost a caller that owns Vm on the host
+ * pays. */
+cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, double* vm_out);
+/* Kernels launched by this engine since creation. */
+cdb_status cdb_engine_launch_count(cdb_engine* e, int64_t* launches);
+/* The CUDA stream (cudaStream_t) the engine launches on. */
+cdb_status cdb_engine_stream(cdb_engine* e, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -220,10 +220,14 @@ void op_sim_step(op_sim_t* s, int nSteps)
                s->iStim[i] = value;
          }
       }
+      /* Cells are independent within each phase, so threading the loops
+       * changes no result. */
+#pragma omp parallel for schedule(static)
       for (int64_t i = 0; i < n; ++i)
          s->dvmR[i] = op_tt06_step(&s->params[s->reaction[i]], s->dt, s->vm[i], s->state + OP_NSTATE * i);
       if (s->useDiffusion) {
          for (int64_t i = 0; i < n; ++i) s->vmBlock[s->blockIndex[i]] = s->vm[i];
+#pragma omp parallel for schedule(static)
          for (int64_t i = 0; i < n; ++i) {
             const double* phi = s->vmBlock + s->blockIndex[i];
             const double* A = s->A + 19 * i;

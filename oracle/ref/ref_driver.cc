@@ -134,7 +134,9 @@ void* ref_sim_create(const char* reactionNames, const char* stimulusNames,
    {
       std::vector<int> ct(cellType, cellType + nCells);
       ro_array_ptr<int> ctp(&ct[0], ct.size());
-      ThreadTeam group = ThreadServer::getInstance().getThreadTeam(std::vector<unsigned>());
+      // The thread server hands each team its own threads and runs out, so
+      // every simulation shares one team (BetterTT06 ignores it).
+      static ThreadTeam group = ThreadServer::getInstance().getThreadTeam(std::vector<unsigned>());
       sim->reaction.create(dt, ctp, group);
    }
    sim->Vm.resize(nCells);

@@ -61,6 +61,24 @@ def compile_objects(text):
     lib().ref_objects_compile(text.encode())
 
 
+_compiled = set()
+_stim_counter = [0]
+
+
+def compile_once(key, text):
+    """The reference's object database is global and merges repeated
+    definitions key by key (values accumulate), so shared objects (fits,
+    reactions) are compiled once per process."""
+    if key not in _compiled:
+        compile_objects(text)
+        _compiled.add(key)
+
+
+def unique_prefix(base="stim"):
+    _stim_counter[0] += 1
+    return "%s%d_" % (base, _stim_counter[0])
+
+
 class RefSim:
     """One tissue on the reference CPU path.  Cells in local order (gid
     order for the synthetic boxes)."""

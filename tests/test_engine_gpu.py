@@ -1,0 +1,209 @@
+"""Parity of the fused B200 engine with the oracle (oracle/port, pinned to
+the reference by tests/test_oracle.py) through the C ABI.
+
+Tolerances (written here, checked below):
+  FP64 path  max |dVm| <= 1e-6 mV after 1000 steps; activation times
+             identical (same step); FGR weights bit-exact; cell-type and
+             index handling bit-exact (each cell keeps its own state).
+  mixed path activation-time error <= 0.5 ms, APD90 error <= 1 ms.
+"""
+import numpy as np
+import pytest
+
+from cardioid_b200 import engine as eng_mod
+from cardioid_b200 import tissue, tt06
+
+pytestmark = pytest.mark.gpu
+
+DT = 0.02
+VM_TOL_FP64 = 1e-6       # mV, after 1000 steps
+ACT_TOL_MIXED = 0.5      # ms
+APD_TOL_MIXED = 1.0      # ms
+
+
+def _reaction_ids(t):
+    return (t.cell_type - 100).astype(np.uint8)
+
+
+def _engine(fits, precision="fp64", graphs=True):
+    e = eng_mod.Engine(DT, precision=precision, use_graphs=graphs)
+    for p in fits:
+        e.add_reaction(p)
+    return e
+
+
+def _masked(nx, ny, nz, seed=3):
+    full = tissue.box(nx, ny, nz, dx=0.2, seed=seed)
+    x, y, z = full.tuples()
+    keep = ~((x >= nx // 3) & (x < 2 * nx // 3) & (y >= ny // 3) & (y < 2 * ny // 3) & (z >= 1) & (z < nz - 1))
+    keep &= ~((x == nx - 1) & (y == 0))
+    return tissue.Tissue(full.nx, full.ny, full.nz, full.dx, full.dy, full.dz, full.gid[keep], full.cell_type[keep],
+                         full.sigma[keep], full.vm0[keep], full.stimuli)
+
+
+@pytest.mark.parametrize("kind", ["box", "cable", "sheet", "masked"])
+def test_weights_bit_exact(cdb_lib, oracle_port, fits002, kind):
+    t = {"box": lambda: tissue.box(12, 10, 8), "cable": lambda: tissue.box(40, 1, 1),
+         "sheet": lambda: tissue.box(20, 16, 1), "masked": lambda: _masked(12, 11, 9)}[kind]()
+    with _engine(fits002) as e:
+        tid = e.add_tissue(t, _reaction_ids(t))
+        w = e.read_weights(tid)
+    ref = oracle_port.PortSim(t, fits002, _reaction_ids(t), DT).weights()
+    np.testing.assert_array_equal(w, ref)
+
+
+@pytest.mark.parametrize("kind,steps", [("box", 1000), ("cable", 1000), ("sheet", 1000), ("masked", 600)])
+def test_fp64_fused_matches_oracle(cdb_lib, oracle_port, fits002, kind, steps):
+    t = {"box": lambda: tissue.box(16, 14, 12), "cable": lambda: tissue.box(300, 1, 1),
+         "sheet": lambda: tissue.box(48, 40, 1), "masked": lambda: _masked(16, 14, 12)}[kind]()
+    rx = _reaction_ids(t)
+    sim = oracle_port.PortSim(t, fits002, rx, DT)
+    with _engine(fits002) as e:
+        tid = e.add_tissue(t, rx)
+        for chunk in (100, 400, steps - 500):
+            e.step(chunk)
+            sim.step(chunk)
+        vm = e.read_vm(tid)
+        act = e.read_activation(tid)
+        states = e.read_states(tid)
+        s, time = e.time(tid)
+    ref = sim.vm()
+    assert s == steps and time == sim.time
+    assert np.abs(vm - ref).max() <= VM_TOL_FP64
+    np.testing.assert_array_equal(act, sim.activation())
+    assert (act > 0).any()
+    rs = sim.states()
+    for k, name in enumerate(tt06.STATE_NAMES):
+        scale = max(1e-12, np.abs(rs[k]).max())
+        assert np.abs(states[k] - rs[k]).max() <= 1e-8 * scale, name
+
+
+def test_config0_fp64_parity_64cubed_1000_steps(cdb_lib, oracle_port, fits002):
+    """The 64^3 box, dt 0.02, 1000 steps, face stimulus at t = 0: max |dVm|
+    <= 1e-6 mV and identical activation times."""
+    t = tissue.box(64, 64, 64)
+    rx = _reaction_ids(t)
+    sim = oracle_port.PortSim(t, fits002, rx, DT)
+    sim.step(1000)
+    with _engine(fits002) as e:
+        tid = e.add_tissue(t, rx)
+        e.step(1000)
+        vm = e.read_vm(tid)
+        act = e.read_activation(tid)
+        lo, hi = e.minmax(tid)
+    assert np.abs(vm - sim.vm()).max() <= VM_TOL_FP64
+    np.testing.assert_array_equal(act, sim.activation())
+    assert lo == vm.min() and hi == vm.max()
+    assert (act > 0).sum() > t.n // 4
+
+
+def test_batched_tissues_equal_alone(cdb_lib, fits002):
+    """Index handling: tissues packed into one launch give bit-identical
+    results to each tissue run alone, per-tissue drug block included."""
+    ts = [tissue.box(20, 1, 1, seed=1), tissue.box(10, 9, 1, seed=2), tissue.box(7, 6, 5, seed=3),
+          _masked(9, 8, 7, seed=4)]
+    scales = [(1.0, 1.0, 1.0), (0.5, 1.0, 1.0), (1.0, 0.3, 0.8), (0.2, 0.9, 0.1)]
+    alone = []
+    for t, sc in zip(ts, scales):
+        with _engine(fits002) as e:
+            tid = e.add_tissue(t, _reaction_ids(t), sc)
+            e.step(300)
+            alone.append((e.read_vm(tid), e.read_states(tid), e.read_activation(tid)))
+    with _engine(fits002) as e:
+        ids = [e.add_tissue(t, _reaction_ids(t), sc) for t, sc in zip(ts, scales)]
+        e.step(300)
+        for tid, (vm, st, act) in zip(ids, alone):
+            np.testing.assert_array_equal(e.read_vm(tid), vm)
+            np.testing.assert_array_equal(e.read_states(tid), st)
+            np.testing.assert_array_equal(e.read_activation(tid), act)
+
+
+def test_join_and_retire_between_steps(cdb_lib, fits002):
+    """A tissue that joins late runs from its own t = 0 and ends equal to the
+    same tissue run alone; retiring one tissue leaves the others unchanged."""
+    a, b = tissue.box(8, 7, 6, seed=5), tissue.box(30, 1, 1, seed=6)
+    with _engine(fits002) as e:
+        ib = e.add_tissue(b, _reaction_ids(b))
+        e.step(200)
+        vb = e.read_vm(ib)
+    with _engine(fits002) as e:
+        ia = e.add_tissue(a, _reaction_ids(a))
+        e.step(150)
+        ib = e.add_tissue(b, _reaction_ids(b))
+        e.step(120)
+        e.remove_tissue(ia)
+        e.step(80)
+        assert e.time(ib)[0] == 200
+        np.testing.assert_array_equal(e.read_vm(ib), vb)
+
+
+def test_graphs_and_plain_launches_agree(cdb_lib, fits002):
+    t = tissue.box(10, 9, 8)
+    out = []
+    for graphs in (True, False):
+        with _engine(fits002, graphs=graphs) as e:
+            tid = e.add_tissue(t, _reaction_ids(t))
+            e.step(37)
+            e.step(37)
+            out.append(e.read_vm(tid))
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_step_host_equals_device_step(cdb_lib, fits002):
+    t = tissue.box(9, 8, 7)
+    with _engine(fits002) as e:
+        tid = e.add_tissue(t, _reaction_ids(t))
+        e.step(5)
+        ref = e.read_vm(tid)
+    with _engine(fits002) as e:
+        tid = e.add_tissue(t, _reaction_ids(t))
+        vm = np.ascontiguousarray(t.vm0, dtype=np.float64)
+        out = np.empty_like(vm)
+        for _ in range(5):
+            e.step_host(tid, vm, out)
+            vm, out = out, vm
+        np.testing.assert_array_equal(vm, ref)
+
+
+def apd90(trace, times):
+    """APD90 per beat of one cell's Vm trace: activation at the first step
+    with Vm > 0, V_rest = Vm just before it, V_peak the maximum after it;
+    repolarisation when Vm first falls below V_rest + 0.1 (V_peak - V_rest)."""
+    up = np.flatnonzero((trace[1:] > 0) & (trace[:-1] <= 0)) + 1
+    out = []
+    for u in up:
+        vrest = trace[u - 1]
+        peak_i = u + np.argmax(trace[u:])
+        thr = vrest + 0.1 * (trace[peak_i] - vrest)
+        below = np.flatnonzero(trace[peak_i:] < thr)
+        if len(below):
+            out.append(times[peak_i + below[0]] - times[u])
+    return np.array(out)
+
+
+def test_mixed_precision_errors_vs_fp64_oracle(cdb_lib, oracle_port, fits002):
+    """Mixed path on a 24x20x16 box for 20000 steps (400 ms, one paced beat):
+    activation-time error <= 0.5 ms, APD90 error <= 1 ms at probe cells."""
+    t = tissue.box(24, 20, 16, period=1000.0)
+    rx = _reaction_ids(t)
+    sim = oracle_port.PortSim(t, fits002, rx, DT)
+    probes = np.array([0, 5, t.n // 3, t.n // 2, t.n - 1])
+    steps, every = 20000, 10
+    tr_o, tr_m, times = [], [], []
+    with _engine(fits002, precision="mixed") as e:
+        tid = e.add_tissue(t, rx)
+        for k in range(0, steps, every):
+            e.step(every)
+            sim.step(every)
+            tr_m.append(e.read_vm(tid)[probes])
+            tr_o.append(sim.vm()[probes])
+            times.append(sim.time)
+        act_m = e.read_activation(tid)
+    act_o = sim.activation()
+    assert ((act_o > 0) == (act_m > 0)).all()
+    assert np.abs(act_m - act_o)[act_o > 0].max() <= ACT_TOL_MIXED
+    tr_o, tr_m, times = np.array(tr_o), np.array(tr_m), np.array(times)
+    for j in range(len(probes)):
+        a_o, a_m = apd90(tr_o[:, j], times), apd90(tr_m[:, j], times)
+        assert len(a_o) == len(a_m) and len(a_o) >= 1
+        assert np.abs(a_o - a_m).max() <= APD_TOL_MIXED

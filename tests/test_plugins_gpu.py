@@ -1,0 +1,90 @@
+"""The drop-in Reaction / Diffusion plugins against the oracle: the same data
+flow as the reference's omp loop (elec/simulationLoop.cc:183-231) driven
+through BetterTT06.calc with an index array and FGRDiffusion.calc."""
+import numpy as np
+import pytest
+
+from cardioid_b200 import objectdb, plugins, tissue
+
+pytestmark = pytest.mark.gpu
+DT = 0.02
+
+
+def test_reaction_plugin_index_gather_scatter(cdb_lib, oracle_port, fits002):
+    """A permuted index array: every cell keeps its own state, dVm lands at
+    indexArray[i] (bit-exact index handling, FP64 values within 1e-9)."""
+    import torch
+    n = 257
+    rng = np.random.default_rng(0)
+    perm = rng.permutation(n).astype(np.int32)
+    vm = -83.0 + rng.uniform(-1, 1, n)
+    t = tissue.Tissue(n, 1, 1, 1.0, 1.0, 1.0, np.arange(n), np.full(n, 101, np.int32), np.zeros((n, 6)), vm, [])
+    sim = oracle_port.PortSim(t, [fits002[1]], np.zeros(n, np.uint8), DT, diffusion=False)
+    r = plugins.BetterTT06(fits002[1], n, DT)
+    idx = torch.from_numpy(perm).cuda()
+    Vm = torch.from_numpy(vm.copy()).cuda()
+    dVm = torch.full((n,), np.nan, dtype=torch.float64, device="cuda")
+    iStim = torch.zeros(n, dtype=torch.float64, device="cuda")
+    for _ in range(50):
+        r.calc(DT, idx, Vm, iStim, dVm)
+        Vm += DT * dVm
+        sim.step(1)
+    torch.cuda.synchronize()
+    got = Vm.cpu().numpy()
+    assert np.abs(got - sim.vm()).max() <= 1e-9
+    st = sim.states()
+    for k in range(18):
+        ours = r.getValues(k)   # reaction-local order: cell i of the reaction is Vm[perm[i]]
+        np.testing.assert_allclose(ours, st[k][perm], rtol=1e-9, atol=1e-15)
+
+
+def test_fgr_plugin_matches_oracle_weights_and_dvm(cdb_lib, oracle_port, fits002):
+    import torch
+    t = tissue.box(11, 9, 7)
+    d = plugins.FGRDiffusion(t)
+    sim = oracle_port.PortSim(t, fits002, (t.cell_type - 100).astype(np.uint8), DT)
+    np.testing.assert_array_equal(d.weights(), sim.weights())
+    sim.step(1)   # dVmD of the first step is computed from vm0
+    Vm = torch.from_numpy(t.vm0.copy()).cuda()
+    dVm = torch.empty_like(Vm)
+    d.updateLocalVoltage(Vm)
+    d.updateRemoteVoltage(None)
+    d.calc(dVm)
+    _, ref, _ = sim.dvm()
+    assert np.abs(dVm.cpu().numpy() - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
+
+
+def test_split_plugins_loop_matches_oracle(cdb_lib, oracle_port, fits002):
+    """ReactionManager + FGRDiffusion + stimulus + integrator, step by step
+    as the omp loop, for 300 steps: within 1e-9 mV of the oracle."""
+    import torch
+    from cardioid_b200 import engine
+    t = tissue.box(10, 8, 6)
+    db = objectdb.ObjectDB()
+    for ct in (0, 1, 2):
+        db.compile_file(engine.shipped_fit_path(DT, ct))
+    db.compile(tissue.reaction_objects_text(["tt06Endo_fit", "tt06Mid_fit", "tt06Epi_fit"]))
+    db.compile("fgr DIFFUSION { method = FGR; diffusionScale = %r; }" % t.diffusion_scale)
+    rm = plugins.ReactionManager(db, ["tt06Endo", "tt06Mid", "tt06Epi"], DT, t.cell_type)
+    diff = plugins.diffusionFactory(db, "fgr", t)
+    sim = oracle_port.PortSim(t, fits002, (t.cell_type - 100).astype(np.uint8), DT)
+    x, y, z = t.tuples()
+    s = t.stimuli[0]
+    inbox = torch.from_numpy((x > s.xMin) & (x < s.xMax) & (y > s.yMin) & (y < s.yMax) & (z > s.zMin) &
+                             (z < s.zMax)).cuda()
+    Vm = torch.from_numpy(t.vm0.copy()).cuda()
+    dVmR, dVmD = torch.zeros_like(Vm), torch.zeros_like(Vm)
+    iStim = torch.zeros_like(Vm)
+    time = 0.0
+    for _ in range(300):
+        iStim.zero_()
+        v = s.value(time)
+        if v != 0:
+            iStim[inbox] = v
+        rm.calc(DT, Vm, iStim, dVmR)
+        diff.updateLocalVoltage(Vm)
+        diff.calc(dVmD)
+        Vm += DT * (dVmR + dVmD + iStim)
+        time += DT
+    sim.step(300)
+    assert np.abs(Vm.cpu().numpy() - sim.vm()).max() <= 1e-9
