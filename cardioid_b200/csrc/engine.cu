@@ -428,12 +428,37 @@ struct HostTissue {
   int nx = 0, ny = 0, nz = 0;
 };
 
+// Constant-memory reaction slots are a per-device resource shared by every
+// engine of the process; each engine takes slots as it registers reaction
+// types and gives them back when destroyed.
+std::mutex g_slot_mutex;
+std::map<int, std::vector<bool>> g_slot_used;
+
+int acquire_slot(int device)
+{
+  std::lock_guard<std::mutex> lock(g_slot_mutex);
+  std::vector<bool>& used = g_slot_used[device];
+  used.resize(CDB_MAX_REACTION_TYPES, false);
+  for (int s = 0; s < CDB_MAX_REACTION_TYPES; ++s)
+    if (!used[s]) {
+      used[s] = true;
+      return s;
+    }
+  return -1;
+}
+
+void release_slot(int device, int slot)
+{
+  std::lock_guard<std::mutex> lock(g_slot_mutex);
+  std::vector<bool>& used = g_slot_used[device];
+  if (slot >= 0 && slot < (int)used.size()) used[slot] = false;
+}
+
 struct Engine {
   cdb_engine_config cfg{};
   cudaStream_t stream = nullptr;
   int nTypes = 0;
-  std::vector<double> coefPool;   // [type][kFitPoolPerType]
-  TypeTables types{};
+  int slots[CDB_MAX_REACTION_TYPES] = {0};   // constant-memory slot of each reaction id
   std::map<int, std::unique_ptr<HostTissue>> tissues;
   int nextId = 0;
   bool dirty = true;
@@ -453,6 +478,7 @@ struct Engine {
     if (graph) cudaGraphExecDestroy(graph);
     tissues.clear();
     if (stream) cudaStreamDestroy(stream);
+    for (int t = 0; t < nTypes; ++t) release_slot(cfg.device, slots[t]);
   }
 
   cdb_status ensure_times(int64_t upto)
@@ -694,7 +720,6 @@ cdb_status cdb_engine_create(const cdb_engine_config* cfg, cdb_engine** out)
   std::unique_ptr<cdb_engine> e(new cdb_engine);
   e->e.cfg = *cfg;
   CDB_CUDA(cudaStreamCreateWithFlags(&e->e.stream, cudaStreamNonBlocking));
-  e->e.coefPool.assign((size_t)CDB_MAX_REACTION_TYPES * kFitPoolPerType, 0.0);
   *out = e.release();
   return CDB_OK;
 }
@@ -714,21 +739,27 @@ cdb_status cdb_engine_add_reaction(cdb_engine* e, const cdb_tt06_params* params,
   CDB_CHECK(e && params && fits && id, CDB_INVALID_ARG, "null argument");
   Engine& E = e->e;
   CDB_CHECK(E.nTypes < CDB_MAX_REACTION_TYPES, CDB_INVALID_ARG, "too many reaction types");
-  const int t = E.nTypes;
+  FitShape shape{};
+  std::vector<double> pool(kFitPoolPerType, 0.0);
   std::string err;
-  double* pool = E.coefPool.data() + (size_t)t * kFitPoolPerType;
-  CDB_CHECK(pack_fits(fits, E.types.shape[t], pool, kFitPoolPerType, err), CDB_INVALID_ARG, err);
-  E.types.scal[t] = to_scalars(*params);
+  CDB_CHECK(pack_fits(fits, shape, pool.data(), kFitPoolPerType, err), CDB_INVALID_ARG, err);
+  const TT06Scalars scal = to_scalars(*params);
   CDB_CUDA(cudaSetDevice(E.cfg.device));
+  const int slot = acquire_slot(E.cfg.device);
+  CDB_CHECK(slot >= 0, CDB_INVALID_ARG,
+            "every constant-memory reaction slot of this device is in use (at most " +
+                std::to_string(CDB_MAX_REACTION_TYPES) + " reaction types across the process's engines)");
+  E.slots[E.nTypes] = slot;
+  E.nTypes += 1;   // the engine owns the slot from here on; destroy releases it
+  std::vector<float> pool32(pool.begin(), pool.end());
   CDB_CUDA(cudaStreamSynchronize(E.stream));
-  std::vector<float> pool32(E.coefPool.size());
-  for (size_t k = 0; k < pool32.size(); ++k) pool32[k] = (float)E.coefPool[k];
-  CDB_CUDA(cudaMemcpyToSymbol(c_scal, E.types.scal, sizeof(E.types.scal)));
-  CDB_CUDA(cudaMemcpyToSymbol(c_shape, E.types.shape, sizeof(E.types.shape)));
-  CDB_CUDA(cudaMemcpyToSymbol(c_coef64, E.coefPool.data(), E.coefPool.size() * sizeof(double)));
-  CDB_CUDA(cudaMemcpyToSymbol(c_coef32, pool32.data(), pool32.size() * sizeof(float)));
-  E.nTypes = t + 1;
-  *id = t;
+  CDB_CUDA(cudaMemcpyToSymbol(c_scal, &scal, sizeof(scal), slot * sizeof(TT06Scalars)));
+  CDB_CUDA(cudaMemcpyToSymbol(c_shape, &shape, sizeof(shape), slot * sizeof(FitShape)));
+  CDB_CUDA(cudaMemcpyToSymbol(c_coef64, pool.data(), pool.size() * sizeof(double),
+                              (size_t)slot * kFitPoolPerType * sizeof(double)));
+  CDB_CUDA(cudaMemcpyToSymbol(c_coef32, pool32.data(), pool32.size() * sizeof(float),
+                              (size_t)slot * kFitPoolPerType * sizeof(float)));
+  *id = E.nTypes - 1;
   return CDB_OK;
 }
 
@@ -825,7 +856,10 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
       CDB_CUDA(cudaMemcpyAsync(h->voxel.p, v.data(), n * 8, cudaMemcpyHostToDevice, s));
       CDB_CUDA(cudaStreamSynchronize(s));
     }
-    CDB_CUDA(cudaMemcpyAsync(h->rtype.p, t->reaction, n, cudaMemcpyHostToDevice, s));
+    // per-cell reaction ids -> this engine's constant-memory slots
+    std::vector<uint8_t> slotOf(n);
+    for (int64_t i = 0; i < n; ++i) slotOf[i] = (uint8_t)E.slots[t->reaction[i]];
+    CDB_CUDA(cudaMemcpyAsync(h->rtype.p, slotOf.data(), n, cudaMemcpyHostToDevice, s));
     CDB_CUDA(cudaStreamSynchronize(s));
   }
   d.vm[0] = h->vm0.as<double>();
