@@ -38,6 +38,9 @@ def workload(name):
         return dict(nx=256, ny=256, nz=256, period=500.0, label="box256: 256^3 = 16,777,216 cells, dx 0.2 mm, "
                     "endo/mid/epi x-slabs 25/35/40 %, fibre -60..+60 deg across z, sigma_l 0.133 / sigma_t 0.0176 S/m, "
                     "beta 1400/cm, Cm 1 uF/cm^2, S1 pacing every 500 ms on the x = 0 face, dt 0.02 ms")
+    if name == "box128":
+        return dict(nx=128, ny=128, nz=128, period=500.0, label="box128: 128^3 = 2,097,152 cells (profiling size), "
+                    "otherwise as box256")
     if name == "box64":
         return dict(nx=64, ny=64, nz=64, period=1000.0, label="box64: 64^3 = 262,144 cells, single stimulus at t = 0 "
                     "on the x = 0 face, otherwise as box256")
@@ -323,7 +326,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["box256", "box64"], default="box256")
+    ap.add_argument("--config", choices=["box256", "box128", "box64"], default="box256")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")

@@ -11,8 +11,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libcardioid_b200.so")
-SOURCES = ["engine.cu", "plugins.cu"]
-HEADERS = ["common.cuh", "tt06_device.cuh", "fgr_device.cuh", os.path.join("..", "..", "include", "cardioid_b200.h")]
+SOURCES = ["engine_host.cu", "plugins.cu"]
+HEADERS = ["common.cuh", "tt06_device.cuh", "fgr_device.cuh", "step_kernel.cuh", "fit_shapes.h",
+           os.path.join("..", "..", "include", "cardioid_b200.h")]
 
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--extended-lambda", "-gencode", "arch=compute_100a,code=sm_100a",
               "-Xcompiler", "-fPIC", "-shared"]

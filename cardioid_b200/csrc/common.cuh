@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 
@@ -46,6 +48,50 @@ struct Status {
     }                                                                                      \
   } while (0)
 
+// Which fits lose accuracy when their monomial Horner form is evaluated in
+// FP32 (as the mixed path does): the FP32 value (FMA Horner, float
+// coefficients) is compared with the FP64 one over the fit's domain (V in
+// [-100, 100] mV; Ca_ss in [1e-7, 0.1] mM for slot 0), and a fit whose
+// largest error exceeds 1e-5 of its largest magnitude is flagged for FP64.
+// High-degree rational fits whose denominator spans many decades (h and m
+// Rush-Larsen rates, the K1 current) are the ones flagged.
+inline uint32_t fp64_fit_mask(const cdb_fit* fits)
+{
+  uint32_t mask = 0;
+  for (int f = 0; f < kNumFits; ++f) {
+    const cdb_fit& F = fits[f];
+    const double lo = f == 0 ? 1e-7 : -100.0, hi = f == 0 ? 0.1 : 100.0;
+    double maxErr = 0, maxVal = 0;
+    const int nPts = 4001;
+    for (int i = 0; i < nPts; ++i) {
+      const double x = lo + (hi - lo) * i / (nPts - 1);
+      double num = F.coeff[F.numer - 1];
+      for (int k = F.numer - 2; k >= 0; --k) num = F.coeff[k] + x * num;
+      double v = num;
+      const float xf = (float)x;
+      float numf = (float)F.coeff[F.numer - 1];
+      for (int k = F.numer - 2; k >= 0; --k) numf = std::fma(xf, numf, (float)F.coeff[k]);
+      float vf = numf;
+      if (F.denom > 1) {
+        const double* d = F.coeff + F.numer;
+        double den = d[F.denom - 2];
+        for (int k = F.denom - 3; k >= 0; --k) den = d[k] + x * den;
+        den = 1 + x * den;
+        v = num / den;
+        float denf = (float)d[F.denom - 2];
+        for (int k = F.denom - 3; k >= 0; --k) denf = std::fma(xf, denf, (float)d[k]);
+        denf = std::fma(xf, denf, 1.0f);
+        vf = numf / denf;
+      }
+      maxVal = std::max(maxVal, std::fabs(v));
+      const double e = std::fabs((double)vf - v);
+      maxErr = std::isfinite(e) ? std::max(maxErr, e) : 1e300;
+    }
+    if (maxErr > 1e-5 * maxVal) mask |= 1u << f;
+  }
+  return mask;
+}
+
 // Packs 30 fits into a coefficient pool; fails when they do not fit.
 inline bool pack_fits(const cdb_fit* fits, FitShape& sh, double* pool, int poolSize, std::string& err)
 {
@@ -65,6 +111,29 @@ inline bool pack_fits(const cdb_fit* fits, FitShape& sh, double* pool, int poolS
     sh.offset[f] = (int16_t)off;
     for (int k = 0; k < nn + nd - 1; ++k) pool[off + k] = fits[f].coeff[k];
     off += nn + nd - 1;
+  }
+  sh.fp64mask = fp64_fit_mask(fits);
+  return true;
+}
+
+// Packs 30 fits at the compile-time offsets of fit_shapes.h, zero-padded,
+// when every fit is no longer than the compiled shape (and needs FP64 in the
+// mixed path only where the compiled kernel uses it); false otherwise.
+inline bool pack_fits_spec(const cdb_fit* fits, double* pool, int poolSize)
+{
+  static_assert(kSpecPool <= kFitPoolPerType, "compiled fit pool exceeds the per-type pool");
+  if ((fp64_fit_mask(fits) & ~kSpecFp64Mask) != 0) return false;
+  for (int f = 0; f < kNumFits; ++f) {
+    const int nn = fits[f].numer, nd = fits[f].denom;
+    if (nn < 1 || nd < 1 || nn > kSpecNumer[f]) return false;
+    if (nd > 1 && nd > kSpecDenom[f]) return false;
+  }
+  for (int k = 0; k < poolSize; ++k) pool[k] = 0.0;
+  for (int f = 0; f < kNumFits; ++f) {
+    const int nn = fits[f].numer, nd = fits[f].denom;
+    const int O = kSpecOffset[f], N = kSpecNumer[f];
+    for (int k = 0; k < nn; ++k) pool[O + k] = fits[f].coeff[k];
+    for (int k = 0; k < nd - 1; ++k) pool[O + N + k] = fits[f].coeff[nn + k];
   }
   return true;
 }

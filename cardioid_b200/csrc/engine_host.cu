@@ -15,9 +15,10 @@
 //              Na_i) and 13 of float (R_prime and the 12 gates);
 //   w          stencil weights, rows x n (FP64: A0 and the class's nodes in
 //              double; mixed: the class's nodes without A0 in float);
-//   rtype      reaction-type byte per cell; voxel (masked tissues only)
-//              int64 padded-voxel index per cell; act activation time.
-// A tile table maps each CTA to kTile consecutive cells of one tissue.
+//   voxel      (masked tissues only) int64 padded-voxel index per cell;
+//   act        activation time per cell.
+// A warp-tile table, grouped by reaction type, maps each warp to up to 32
+// consecutive cells of one tissue and one reaction type (step_kernel.cuh).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -29,369 +30,13 @@
 
 #include "common.cuh"
 #include "fgr_device.cuh"
+#include "step_kernel.cuh"
 
 namespace cdb {
 
 thread_local std::string t_last_error;
 void set_error(const std::string& msg) { t_last_error = msg; }
 int64_t g_launches = 0;
-
-constexpr int kTile = 128;
-
-__constant__ TT06Scalars c_scal[CDB_MAX_REACTION_TYPES];
-__constant__ FitShape c_shape[CDB_MAX_REACTION_TYPES];
-__constant__ double c_coef64[CDB_MAX_REACTION_TYPES * kFitPoolPerType];
-__constant__ float c_coef32[CDB_MAX_REACTION_TYPES * kFitPoolPerType];
-
-struct TissueDev {
-  double* vm[2];
-  double* s64;
-  float* s32;
-  const void* w;
-  const uint8_t* rtype;
-  const int64_t* voxel;
-  double* act;
-  int64_t n;
-  int64_t px, pxy;        // padded strides
-  int nx, ny, nz;
-  int py0, pz0;           // 1 when y (z) is padded
-  int cls;
-  int nstim, stim0;
-  int parity;             // buffer holding Vm at the start of the next launch batch
-  int64_t step0;          // steps taken at the start of the next launch batch
-  double scale;           // diffusionScale (0: no diffusion)
-  BlockScale blk;
-  unsigned long long* minmax;   // 2 slots
-};
-
-struct Tile {
-  int tissue;
-  int count;
-  int64_t first;
-};
-
-struct StepArgs {
-  TissueDev* tissues;
-  const Tile* tiles;
-  const cdb_stimulus* stims;
-  const double* times;
-  double dt;
-  int k;                  // step within the launch batch
-  int minmax;             // reduce min/max this step
-};
-
-__device__ __forceinline__ double pulse_value(const cdb_stimulus& s, double time)
-{
-  if (!(time > s.t0 && time < s.tf)) return 0.0;
-  const double t = time - floor(time / s.period) * s.period;
-  return (t >= s.phase && t < s.phase + s.duration) ? s.amplitude : 0.0;
-}
-
-// Geometry of one tissue, held in registers by the step kernel.
-struct Geom {
-  const int64_t* voxel;
-  int64_t px, pxy;
-  int nx, ny, py0, pz0;
-};
-
-__device__ __forceinline__ void cell_coords(const Geom& g, int64_t i, int64_t& vox, int& x, int& y, int& z)
-{
-  if (g.voxel) {
-    vox = g.voxel[i];
-    const int64_t yz = vox / g.px;
-    x = (int)(vox - yz * g.px) - 1;
-    const int64_t py = g.pxy / g.px;
-    const int64_t zz = yz / py;
-    y = (int)(yz - zz * py) - g.py0;
-    z = (int)zz - g.pz0;
-  } else {
-    const int nxy = g.nx * g.ny;
-    const int ii = (int)i;
-    z = ii / nxy;
-    const int r = ii - z * nxy;
-    y = r / g.nx;
-    x = r - y * g.nx;
-    vox = (int64_t)(x + 1) + g.px * (int64_t)(y + g.py0) + g.pxy * (int64_t)(z + g.pz0);
-  }
-}
-
-__device__ __forceinline__ int64_t node_offset(int64_t px, int64_t pxy, int node)
-{
-  return (int64_t)node_dx(node) + px * node_dy(node) + pxy * node_dz(node);
-}
-
-// FP64 stencil in the reference's order: A0 phi0 + sum_k A_k phi_k.
-template <int CLS>
-__device__ __forceinline__ double stencil64(const double* __restrict__ w, int64_t n, int64_t px, int64_t pxy,
-                                            const double* __restrict__ vin, int64_t vox, double phi0, int64_t i)
-{
-  double tmp = __ldg(w + i) * phi0;
-#pragma unroll
-  for (int r = 1; r < class_rows(CLS); ++r) {
-    const int node = class_node(CLS, r);
-    tmp += __ldg(w + r * n + i) * __ldg(vin + vox + node_offset(px, pxy, node));
-  }
-  return tmp;
-}
-
-// Mixed stencil: sum_k A_k (phi_k - phi0) with FP32 weights; the
-// differences are taken in FP64 (A0 = -sum A_k).
-template <int CLS>
-__device__ __forceinline__ double stencil32(const float* __restrict__ w, int64_t n, int64_t px, int64_t pxy,
-                                            const double* __restrict__ vin, int64_t vox, double phi0, int64_t i)
-{
-  float tmp = 0.f;
-#pragma unroll
-  for (int r = 1; r < class_rows(CLS); ++r) {
-    const int node = class_node(CLS, r);
-    const float d = (float)(__ldg(vin + vox + node_offset(px, pxy, node)) - phi0);
-    tmp = fmaf(__ldg(w + (r - 1) * n + i), d, tmp);
-  }
-  return (double)tmp;
-}
-
-template <bool MIXED>
-__global__ void __launch_bounds__(kTile) fused_step_kernel(StepArgs a)
-{
-  __shared__ cdb_stimulus s_stim[CDB_MAX_STIM_PER_TISSUE];
-  __shared__ double s_val[CDB_MAX_STIM_PER_TISSUE];
-  const Tile tile = a.tiles[blockIdx.x];
-  const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
-  const int64_t lstep = Tp->step0 + a.k;
-  const double time = a.times[lstep];
-  const double tnext = a.times[lstep + 1];
-  const int nstim = Tp->nstim;
-  if (threadIdx.x < nstim) {
-    s_stim[threadIdx.x] = a.stims[Tp->stim0 + threadIdx.x];
-    s_val[threadIdx.x] = pulse_value(s_stim[threadIdx.x], time);
-  }
-  __syncthreads();
-  const bool active = threadIdx.x < tile.count;
-  double vnew = 0.0;
-  if (active) {
-    const int64_t i = tile.first + threadIdx.x;
-    const int cur = (Tp->parity + a.k) & 1;
-    const double* __restrict__ vin = Tp->vm[cur];
-    double* __restrict__ vout = Tp->vm[cur ^ 1];
-    Geom g;
-    g.voxel = Tp->voxel; g.px = Tp->px; g.pxy = Tp->pxy; g.nx = Tp->nx; g.ny = Tp->ny;
-    g.py0 = Tp->py0; g.pz0 = Tp->pz0;
-    const int64_t n = Tp->n;   // tissues hold fewer than 2^31 cells
-    const double scale = Tp->scale;
-    const int cls = Tp->cls;
-    const void* wp = Tp->w;
-    const BlockScale blk = Tp->blk;
-    double* const s64base = Tp->s64;
-    float* const s32base = Tp->s32;
-    double* const act = Tp->act;
-    const int rt = Tp->rtype[i];
-    int64_t vox;
-    int x, y, z;
-    cell_coords(g, i, vox, x, y, z);
-    const double phi0 = vin[vox];
-
-    double dvmD = 0.0;
-    if (scale != 0.0) {
-      double acc;
-      if (MIXED) {
-        const float* w = (const float*)wp;
-        acc = cls == kVolume ? stencil32<kVolume>(w, n, g.px, g.pxy, vin, vox, phi0, i)
-            : cls == kSheet ? stencil32<kSheet>(w, n, g.px, g.pxy, vin, vox, phi0, i)
-                            : stencil32<kCable>(w, n, g.px, g.pxy, vin, vox, phi0, i);
-      } else {
-        const double* w = (const double*)wp;
-        acc = cls == kVolume ? stencil64<kVolume>(w, n, g.px, g.pxy, vin, vox, phi0, i)
-            : cls == kSheet ? stencil64<kSheet>(w, n, g.px, g.pxy, vin, vox, phi0, i)
-                            : stencil64<kCable>(w, n, g.px, g.pxy, vin, vox, phi0, i);
-      }
-      dvmD = acc * scale;
-    }
-
-    double dvmR;
-    if (MIXED) {
-      double* s64 = s64base + i;
-      float* s32 = s32base + i;
-      CellState<float> st;
-      st.caSR = s64[0 * n]; st.caI = s64[1 * n]; st.caSS = s64[2 * n];
-      st.kI = s64[3 * n]; st.naI = s64[4 * n];
-      st.rPrime = s32[0 * n]; st.Xr1 = s32[1 * n]; st.Xr2 = s32[2 * n];
-      st.Xs = s32[3 * n]; st.d = s32[4 * n]; st.f = s32[5 * n];
-      st.f2 = s32[6 * n]; st.fCass = s32[7 * n]; st.h = s32[8 * n];
-      st.j = s32[9 * n]; st.m = s32[10 * n]; st.r = s32[11 * n];
-      st.s = s32[12 * n];
-      dvmR = (double)tt06_step_mixed(c_scal[rt], blk, c_coef32 + rt * kFitPoolPerType, c_shape[rt],
-                                     (float)a.dt, a.dt, phi0, st);
-      s64[0 * n] = st.caSR; s64[1 * n] = st.caI; s64[2 * n] = st.caSS;
-      s64[3 * n] = st.kI; s64[4 * n] = st.naI;
-      s32[0 * n] = st.rPrime; s32[1 * n] = st.Xr1; s32[2 * n] = st.Xr2;
-      s32[3 * n] = st.Xs; s32[4 * n] = st.d; s32[5 * n] = st.f;
-      s32[6 * n] = st.f2; s32[7 * n] = st.fCass; s32[8 * n] = st.h;
-      s32[9 * n] = st.j; s32[10 * n] = st.m; s32[11 * n] = st.r;
-      s32[12 * n] = st.s;
-    } else {
-      double* s = s64base + i;
-      CellState<double> st;
-      st.caSR = s[S_Ca_SR * n]; st.caI = s[S_Ca_i * n]; st.caSS = s[S_Ca_ss * n];
-      st.kI = s[S_K_i * n]; st.naI = s[S_Na_i * n]; st.rPrime = s[S_R_prime * n];
-      st.Xr1 = s[S_Xr1 * n]; st.Xr2 = s[S_Xr2 * n]; st.Xs = s[S_Xs * n];
-      st.d = s[S_d * n]; st.f = s[S_f * n]; st.f2 = s[S_f2 * n];
-      st.fCass = s[S_fCass * n]; st.h = s[S_h * n]; st.j = s[S_j * n];
-      st.m = s[S_m * n]; st.r = s[S_r * n]; st.s = s[S_s * n];
-      dvmR = tt06_step(c_scal[rt], blk, c_coef64 + rt * kFitPoolPerType, c_shape[rt], a.dt, phi0, st);
-      s[S_Ca_SR * n] = st.caSR; s[S_Ca_i * n] = st.caI; s[S_Ca_ss * n] = st.caSS;
-      s[S_K_i * n] = st.kI; s[S_Na_i * n] = st.naI; s[S_R_prime * n] = st.rPrime;
-      s[S_Xr1 * n] = st.Xr1; s[S_Xr2 * n] = st.Xr2; s[S_Xs * n] = st.Xs;
-      s[S_d * n] = st.d; s[S_f * n] = st.f; s[S_f2 * n] = st.f2;
-      s[S_fCass * n] = st.fCass; s[S_h * n] = st.h; s[S_j * n] = st.j;
-      s[S_m * n] = st.m; s[S_r * n] = st.r; s[S_s * n] = st.s;
-    }
-
-    double istim = 0.0;
-    for (int k = 0; k < nstim; ++k) {
-      const double v = s_val[k];
-      if (v != 0.0) {
-        const cdb_stimulus& b = s_stim[k];
-        if (x > b.xMin && x < b.xMax && y > b.yMin && y < b.yMax && z > b.zMin && z < b.zMax) istim = v;
-      }
-    }
-    vnew = phi0 + a.dt * (dvmR + dvmD + istim);
-    vout[vox] = vnew;
-    if (vnew > 0.0) {
-      double* ap = act + i;
-      if (*ap < 0.0) *ap = tnext;
-    }
-  }
-  if (a.minmax) {
-    double lo = active ? vnew : __longlong_as_double(0x7ff0000000000000ll);
-    double hi = active ? vnew : -__longlong_as_double(0x7ff0000000000000ll);
-    for (int o = 16; o > 0; o >>= 1) {
-      lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    }
-    if ((threadIdx.x & 31) == 0 && (threadIdx.x < tile.count)) {
-      atomicMin(Tp->minmax, ordered_bits(lo));
-      atomicMax(Tp->minmax + 1, ordered_bits(hi));
-    }
-  }
-}
-
-// After a launch batch of k steps: every tissue is k steps further.
-__global__ void advance_kernel(TissueDev* tissues, int nTissues, int k)
-{
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < nTissues) {
-    tissues[t].step0 += k;
-    tissues[t].parity = (tissues[t].parity + k) & 1;
-  }
-}
-
-__global__ void reset_minmax_kernel(TissueDev* tissues, int nTissues)
-{
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < nTissues) {
-    tissues[t].minmax[0] = ordered_bits(__longlong_as_double(0x7ff0000000000000ll));
-    tissues[t].minmax[1] = ordered_bits(-__longlong_as_double(0x7ff0000000000000ll));
-  }
-}
-
-// ---- set-up kernels ----
-
-// Marks tissue voxels of the full-padded build block with their cell index.
-__global__ void build_voxel_map_kernel(int64_t n, const int64_t* __restrict__ gid, int nx, int ny, int64_t bx,
-                                       int64_t bxy, int64_t* __restrict__ map, int64_t* __restrict__ cellVoxel)
-{
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int64_t g = gid ? gid[i] : i;
-  const int64_t x = g % nx, y = (g / nx) % ny, z = g / ((int64_t)nx * ny);
-  const int64_t v = (x + 1) + bx * (y + 1) + bxy * (z + 1);
-  map[v] = i;
-  cellVoxel[i] = v;
-}
-
-// Weights of every cell (fgr_cell_weights), written in the tissue's class
-// layout: FP64 rows = A0 then the class nodes; mixed rows = class nodes.
-__global__ void build_weights_kernel(int64_t n, const int64_t* __restrict__ map, const int64_t* __restrict__ cellVoxel,
-                                     const double* __restrict__ sigma6, int64_t bx, int64_t bxy, double hx, double hy,
-                                     double hz, int cls, int mixed, void* __restrict__ wout,
-                                     double* __restrict__ w19)
-{
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int64_t v = cellVoxel[i];
-  int tissue[19];
-  int64_t nbrCell[19];
-  for (int k = 0; k < 19; ++k) {
-    const int64_t c = map[v + node_dx(k) + bx * node_dy(k) + bxy * node_dz(k)];
-    nbrCell[k] = c;
-    tissue[k] = c >= 0;
-  }
-  double W[19];
-  fgr_cell_weights(tissue, [&](int k, int c) { return sigma6[6 * nbrCell[k] + c]; }, hx, hy, hz, W);
-  const int rows = class_rows(cls);
-  if (mixed) {
-    float* w = (float*)wout;
-    for (int r = 1; r < rows; ++r) w[(r - 1) * n + i] = (float)W[class_node(cls, r)];
-  } else {
-    double* w = (double*)wout;
-    w[i] = W[0];
-    for (int r = 1; r < rows; ++r) w[r * n + i] = W[class_node(cls, r)];
-  }
-  if (w19)
-    for (int k = 0; k < 19; ++k) w19[k * n + i] = W[k];
-}
-
-// Scatter / gather between cell order and the padded block.
-__global__ void scatter_vm_kernel(int64_t n, const double* __restrict__ src, double* __restrict__ blk,
-                                  const int64_t* __restrict__ voxel, int nx, int ny, int64_t px, int64_t pxy, int py0,
-                                  int pz0)
-{
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int64_t v;
-  if (voxel) v = voxel[i];
-  else {
-    const int64_t x = i % nx, y = (i / nx) % ny, z = i / ((int64_t)nx * ny);
-    v = (x + 1) + px * (y + py0) + pxy * (z + pz0);
-  }
-  blk[v] = src[i];
-}
-
-__global__ void gather_vm_kernel(int64_t n, const double* __restrict__ blk, double* __restrict__ dst,
-                                 const int64_t* __restrict__ voxel, int nx, int ny, int64_t px, int64_t pxy, int py0,
-                                 int pz0)
-{
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int64_t v;
-  if (voxel) v = voxel[i];
-  else {
-    const int64_t x = i % nx, y = (i / nx) % ny, z = i / ((int64_t)nx * ny);
-    v = (x + 1) + px * (y + py0) + pxy * (z + pz0);
-  }
-  dst[i] = blk[v];
-}
-
-__global__ void init_state_kernel(int64_t n, double* s64, float* s32, int mixed, double* act)
-{
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (mixed) {
-    for (int k = 0; k < 5; ++k) s64[k * n + i] = tt06_initial_state(k);
-    for (int k = 5; k < kNumStates; ++k) s32[(k - 5) * n + i] = (float)tt06_initial_state(k);
-  } else {
-    for (int k = 0; k < kNumStates; ++k) s64[k * n + i] = tt06_initial_state(k);
-  }
-  act[i] = -1.0;
-}
-
-__global__ void fill_kernel(int64_t n, double* p, double v)
-{
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) p[i] = v;
-}
-
-inline unsigned grid_for(int64_t n, int block) { return (unsigned)((n + block - 1) / block); }
 
 // ---- host engine ----
 
@@ -421,7 +66,8 @@ struct DeviceBuffer {
 struct HostTissue {
   TissueDev dev{};
   std::vector<cdb_stimulus> stims;
-  DeviceBuffer vm0, vm1, s64, s32, w, rtype, voxel, act, minmax;
+  DeviceBuffer vm0, vm1, s64, s32, w, voxel, act, minmax;
+  std::vector<uint8_t> slotOf;   // constant-memory slot of each cell
   int64_t steps = 0;       // steps taken
   int parity = 0;
   int64_t n = 0;
@@ -459,6 +105,7 @@ struct Engine {
   cudaStream_t stream = nullptr;
   int nTypes = 0;
   int slots[CDB_MAX_REACTION_TYPES] = {0};   // constant-memory slot of each reaction id
+  bool spec[CDB_MAX_REACTION_TYPES] = {false};   // slot packed for the compiled fit shapes
   std::map<int, std::unique_ptr<HostTissue>> tissues;
   int nextId = 0;
   bool dirty = true;
@@ -467,6 +114,7 @@ struct Engine {
   std::vector<double> times{0.0};
   std::vector<int> order;         // tissue ids in table order
   int64_t nTiles = 0;
+  std::vector<std::pair<int, std::pair<int, int>>> slotTiles;   // slot -> (first tile, tile count)
   int64_t launches = 0;
   // graph of a launch batch
   cudaGraphExec_t graph = nullptr;
@@ -503,7 +151,8 @@ struct Engine {
     CDB_CUDA(cudaStreamSynchronize(stream));
     order.clear();
     std::vector<TissueDev> devs;
-    std::vector<Tile> tiles;
+    std::vector<WarpTile> tiles;
+    std::vector<WarpTile> bySlot[CDB_MAX_REACTION_TYPES];
     std::vector<cdb_stimulus> stims;
     for (auto& kv : tissues) {
       HostTissue& t = *kv.second;
@@ -515,22 +164,34 @@ struct Engine {
       const int idx = (int)devs.size();
       devs.push_back(t.dev);
       order.push_back(kv.first);
-      for (int64_t f = 0; f < t.n; f += kTile) {
-        Tile tl;
+      // runs of one reaction type, cut into warp tiles of at most 32 cells
+      int64_t f = 0;
+      while (f < t.n) {
+        const uint8_t slot = t.slotOf[f];
+        int64_t e = f + 1;
+        while (e < t.n && e - f < 32 && t.slotOf[e] == slot) ++e;
+        WarpTile tl;
         tl.tissue = idx;
         tl.first = f;
-        tl.count = (int)std::min<int64_t>(kTile, t.n - f);
-        tiles.push_back(tl);
+        tl.count = (int)(e - f);
+        bySlot[slot].push_back(tl);
+        f = e;
       }
+    }
+    slotTiles.clear();
+    for (int sl = 0; sl < CDB_MAX_REACTION_TYPES; ++sl) {
+      if (bySlot[sl].empty()) continue;
+      slotTiles.push_back({sl, {(int)tiles.size(), (int)bySlot[sl].size()}});
+      tiles.insert(tiles.end(), bySlot[sl].begin(), bySlot[sl].end());
     }
     nTiles = (int64_t)tiles.size();
     CDB_CUDA(dTissues.alloc(std::max<size_t>(1, devs.size()) * sizeof(TissueDev)));
-    CDB_CUDA(dTiles.alloc(std::max<size_t>(1, tiles.size()) * sizeof(Tile)));
+    CDB_CUDA(dTiles.alloc(std::max<size_t>(1, tiles.size()) * sizeof(WarpTile)));
     CDB_CUDA(dStims.alloc(std::max<size_t>(1, stims.size()) * sizeof(cdb_stimulus)));
     if (!devs.empty())
       CDB_CUDA(cudaMemcpy(dTissues.p, devs.data(), devs.size() * sizeof(TissueDev), cudaMemcpyHostToDevice));
     if (!tiles.empty())
-      CDB_CUDA(cudaMemcpy(dTiles.p, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+      CDB_CUDA(cudaMemcpy(dTiles.p, tiles.data(), tiles.size() * sizeof(WarpTile), cudaMemcpyHostToDevice));
     if (!stims.empty())
       CDB_CUDA(cudaMemcpy(dStims.p, stims.data(), stims.size() * sizeof(cdb_stimulus), cudaMemcpyHostToDevice));
     if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
@@ -555,19 +216,28 @@ struct Engine {
       ++launches;
     }
     for (int s = 0; s < k; ++s) {
-      StepArgs a;
-      a.tissues = dTissues.as<TissueDev>();
-      a.tiles = dTiles.as<Tile>();
-      a.stims = dStims.as<cdb_stimulus>();
-      a.times = dTimes.as<double>();
-      a.dt = cfg.dt;
-      a.k = s;
-      a.minmax = (minmax && s == k - 1) ? 1 : 0;
-      if (cfg.precision == CDB_MIXED)
-        fused_step_kernel<true><<<(unsigned)nTiles, kTile, 0, stream>>>(a);
-      else
-        fused_step_kernel<false><<<(unsigned)nTiles, kTile, 0, stream>>>(a);
-      ++launches;
+      for (const auto& st : slotTiles) {
+        StepArgs a;
+        a.tissues = dTissues.as<TissueDev>();
+        a.tiles = dTiles.as<WarpTile>() + st.second.first;
+        a.nTiles = st.second.second;
+        a.rt = st.first;
+        a.stims = dStims.as<cdb_stimulus>();
+        a.times = dTimes.as<double>();
+        a.dt = cfg.dt;
+        a.k = s;
+        a.minmax = (minmax && s == k - 1) ? 1 : 0;
+        const unsigned grid = grid_for(a.nTiles, kWarpsPerCta);
+        const bool sp = spec[st.first];
+        if (cfg.precision == CDB_MIXED) {
+          if (sp) fused_step_kernel<true, true><<<grid, kCta, 0, stream>>>(a);
+          else fused_step_kernel<true, false><<<grid, kCta, 0, stream>>>(a);
+        } else {
+          if (sp) fused_step_kernel<false, true><<<grid, kCta, 0, stream>>>(a);
+          else fused_step_kernel<false, false><<<grid, kCta, 0, stream>>>(a);
+        }
+        ++launches;
+      }
     }
     advance_kernel<<<grid_for(nT, 128), 128, 0, stream>>>(dTissues.as<TissueDev>(), nT, k);
     ++launches;
@@ -684,7 +354,7 @@ int64_t tissue_bytes(const Engine& E, const cdb_tissue_desc* t)
   int64_t b = 2 * vox * 8;                                   // Vm blocks
   b += mixed ? n * (5 * 8 + 13 * 4) : n * 18 * 8;           // state
   b += mixed ? n * (class_rows(cls) - 1) * 4 : n * class_rows(cls) * 8;   // weights
-  b += n + n * 8 + (masked ? n * 8 : 0) + 64;               // rtype, act, voxel
+  b += n * 8 + (masked ? n * 8 : 0) + 64;                   // act, voxel
   return b;
 }
 
@@ -743,6 +413,8 @@ cdb_status cdb_engine_add_reaction(cdb_engine* e, const cdb_tt06_params* params,
   std::vector<double> pool(kFitPoolPerType, 0.0);
   std::string err;
   CDB_CHECK(pack_fits(fits, shape, pool.data(), kFitPoolPerType, err), CDB_INVALID_ARG, err);
+  // fits no longer than the compiled shapes run the unrolled kernel
+  const bool specialised = pack_fits_spec(fits, pool.data(), kFitPoolPerType);
   const TT06Scalars scal = to_scalars(*params);
   CDB_CUDA(cudaSetDevice(E.cfg.device));
   const int slot = acquire_slot(E.cfg.device);
@@ -750,6 +422,7 @@ cdb_status cdb_engine_add_reaction(cdb_engine* e, const cdb_tt06_params* params,
             "every constant-memory reaction slot of this device is in use (at most " +
                 std::to_string(CDB_MAX_REACTION_TYPES) + " reaction types across the process's engines)");
   E.slots[E.nTypes] = slot;
+  E.spec[slot] = specialised;
   E.nTypes += 1;   // the engine owns the slot from here on; destroy releases it
   std::vector<float> pool32(pool.begin(), pool.end());
   CDB_CUDA(cudaStreamSynchronize(E.stream));
@@ -819,7 +492,6 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
   }
   const int rows = class_rows(cls);
   CDB_CUDA(h->w.alloc(mixed ? n * (rows - 1) * 4 : n * rows * 8));
-  CDB_CUDA(h->rtype.alloc(n));
   CDB_CUDA(h->act.alloc(n * 8));
   CDB_CUDA(h->minmax.alloc(16));
   if (masked) CDB_CUDA(h->voxel.alloc(n * 8));
@@ -842,7 +514,7 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
                                                             map.as<int64_t>(), cellVoxel.as<int64_t>());
     build_weights_kernel<<<grid_for(n, 128), 128, 0, s>>>(n, map.as<int64_t>(), cellVoxel.as<int64_t>(),
                                                           sig.as<double>(), bx, bxy, t->dx, t->dy, t->dz, cls,
-                                                          mixed ? 1 : 0, h->w.p, nullptr);
+                                                          mixed ? 1 : 0, h->w.p);
     E.launches += 2;
     if (masked) {
       // cell voxels in the engine's (class-padded) block; masked tissues are kVolume
@@ -857,9 +529,8 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
       CDB_CUDA(cudaStreamSynchronize(s));
     }
     // per-cell reaction ids -> this engine's constant-memory slots
-    std::vector<uint8_t> slotOf(n);
-    for (int64_t i = 0; i < n; ++i) slotOf[i] = (uint8_t)E.slots[t->reaction[i]];
-    CDB_CUDA(cudaMemcpyAsync(h->rtype.p, slotOf.data(), n, cudaMemcpyHostToDevice, s));
+    h->slotOf.resize(n);
+    for (int64_t i = 0; i < n; ++i) h->slotOf[i] = (uint8_t)E.slots[t->reaction[i]];
     CDB_CUDA(cudaStreamSynchronize(s));
   }
   d.vm[0] = h->vm0.as<double>();
@@ -867,7 +538,6 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
   d.s64 = h->s64.as<double>();
   d.s32 = h->s32.as<float>();
   d.w = h->w.p;
-  d.rtype = h->rtype.as<uint8_t>();
   d.voxel = masked ? h->voxel.as<int64_t>() : nullptr;
   d.act = h->act.as<double>();
   d.minmax = h->minmax.as<unsigned long long>();

@@ -47,7 +47,8 @@ __global__ void __launch_bounds__(128) reaction_calc_kernel(ReactionArgs a, doub
     float* g = &st.rPrime;
     // R_prime then the 12 gates, contiguous in CellState<float>
     for (int k = 0; k < 13; ++k) g[k] = s32[k * n];
-    dVm[e] = (double)tt06_step_mixed(a.p, none, a.coef32, a.sh, (float)dt, dt, V, st);
+    GenericFits fits{a.coef64, a.coef32, &a.sh};
+    dVm[e] = (double)tt06_step_mixed(a.p, none, fits, (float)dt, V, st);
     s64[0] = st.caSR; s64[n] = st.caI; s64[2 * n] = st.caSS; s64[3 * n] = st.kI; s64[4 * n] = st.naI;
     for (int k = 0; k < 13; ++k) s32[k * n] = g[k];
   } else {
@@ -56,7 +57,8 @@ __global__ void __launch_bounds__(128) reaction_calc_kernel(ReactionArgs a, doub
     st.caSR = s[0]; st.caI = s[n]; st.caSS = s[2 * n]; st.kI = s[3 * n]; st.naI = s[4 * n];
     double* g = &st.rPrime;
     for (int k = 0; k < 13; ++k) g[k] = s[(5 + k) * n];
-    dVm[e] = tt06_step(a.p, none, a.coef64, a.sh, dt, V, st);
+    GenericFits fits{a.coef64, nullptr, &a.sh};
+    dVm[e] = tt06_step(a.p, none, fits, dt, V, st);
     s[0] = st.caSR; s[n] = st.caI; s[2 * n] = st.caSS; s[3 * n] = st.kI; s[4 * n] = st.naI;
     for (int k = 0; k < 13; ++k) s[(5 + k) * n] = g[k];
   }

@@ -6,15 +6,21 @@
 // currents, forward Euler on Ca_SR, Ca_i, Ca_ss, K_i, Na_i, R_prime and
 // Rush-Larsen (X += a*(X + b)) on 12 gates; returns dVm = -Iion.
 //
-// Two precisions share this code through the Real template argument:
-//   Real = double : the FP64 path; every operation in double, expressions in
-//                   the reference's order (the compiler may contract a*b+c
-//                   into an FMA, which only changes the last bit).
-//   Real = float  : the mixed path; fits, gates, currents and R_prime in
-//                   FP32, the five concentrations and Vm in FP64 (their
-//                   per-step increments are ~1e-7 of their values).
+// Two precisions:
+//   tt06_step        FP64; every operation in double, expressions in the
+//                    reference's order (the compiler contracts a*b+c into an
+//                    FMA, which only changes last bits).
+//   tt06_step_mixed  fits, gates, currents and R_prime in FP32; Vm and the
+//                    five concentrations in FP64 (their per-step increments
+//                    are ~1e-7 of their values); the few fits whose monomial
+//                    form loses accuracy in FP32 are evaluated in FP64.
+// Fit evaluation is a policy: GenericFits reads term counts at run time;
+// SpecFits has them as compile-time constants (fit_shapes.h), so every
+// Horner chain unrolls and the 30 independent chains interleave.
 #pragma once
 #include <cstdint>
+
+#include "fit_shapes.h"
 
 namespace cdb {
 
@@ -22,7 +28,6 @@ constexpr int kNumFits = 30;
 constexpr int kNumStates = 18;
 constexpr int kMaxCoeff = 64;        // per fit (numer + denom - 1 <= 63)
 constexpr int kMaxReactionTypes = 8;
-constexpr int kFitPool = 2048;       // coefficients per reaction type
 
 // Fit slots, in the order of the reference's _interpolant[] (elec/BetterTT06.cc:35-66).
 enum FitSlot {
@@ -48,6 +53,9 @@ struct FitShape {
   int16_t numer[kNumFits];
   int16_t denom[kNumFits];
   int16_t offset[kNumFits];
+  // Fits the mixed path evaluates in FP64: those whose monomial Horner form
+  // loses more than 1e-5 of their range in FP32 (set at registration).
+  uint32_t fp64mask;
 };
 
 // Per-tissue multipliers of the unfitted conductances (drug block).
@@ -55,23 +63,8 @@ struct BlockScale {
   float g_Kr, g_CaL, g_Na;
 };
 
-template <typename Real>
-struct Consts;
-
-template <>
-struct Consts<double> {
-  static constexpr double Cm = 0.185, F = 96485.3415, R = 8314.472, T = 310;
-  static constexpr double Vc = 0.016404, Cao = 2, BufC = 0.2, BufSr = 10, BufSs = 0.4, EC = 1.5;
-  static constexpr double KbufC = 0.001, KbufSr = 0.3, KbufSs = 0.00025, Kup = 0.00025;
-  static constexpr double Vleak = 0.00036, Vrel = 0.102, Vsr = 0.001094, Vss = 5.468e-5;
-  static constexpr double Vxfer = 0.0038, VmaxUp = 0.006375, K1p = 0.15, K2p = 0.045, K3 = 0.06;
-  static constexpr double K4 = 0.005, MaxSr = 2.5, MinSr = 1, KpCa = 0.0005, KNaCa = 1000;
-  static constexpr double Ksat = 0.1, KmCa = 1.38, KmNai = 87.5, Alpha = 2.5, Ko = 5.4;
-  static constexpr double Pkna = 0.03, Nao = 140, KmNa = 40;
-};
-
 // Horner numerator over (1 + x * Horner denominator); the monomial form
-// written by the fit generator (elec/Interpolation.hh:11-99).
+// of the FIT files (elec/Interpolation.hh:11-99).
 template <typename Real>
 __device__ __forceinline__ Real fit_eval(const Real* __restrict__ c, int numer, int denom, Real x)
 {
@@ -101,21 +94,94 @@ __device__ __forceinline__ float fit_eval_fast(const float* __restrict__ c, int 
   return __fdividef(num, den);
 }
 
-// The gate and state vector of one cell: concentrations in double, the
-// other 13 in Real.
+// The same with compile-time term counts and offsets (fully unrolled).
+template <int SLOT>
+__device__ __forceinline__ double fit_spec64(const double* __restrict__ c, double x)
+{
+  constexpr int N = kSpecNumer[SLOT], D = kSpecDenom[SLOT], O = kSpecOffset[SLOT];
+  double num = c[O + N - 1];
+#pragma unroll
+  for (int k = N - 2; k >= 0; --k) num = c[O + k] + x * num;
+  if (D == 1) return num;
+  double den = c[O + N + D - 2];
+#pragma unroll
+  for (int k = D - 3; k >= 0; --k) den = c[O + N + k] + x * den;
+  den = 1.0 + x * den;
+  return num / den;
+}
+
+template <int SLOT>
+__device__ __forceinline__ float fit_spec32(const float* __restrict__ c, float x)
+{
+  constexpr int N = kSpecNumer[SLOT], D = kSpecDenom[SLOT], O = kSpecOffset[SLOT];
+  float num = c[O + N - 1];
+#pragma unroll
+  for (int k = N - 2; k >= 0; --k) num = fmaf(x, num, c[O + k]);
+  if (D == 1) return num;
+  float den = c[O + N + D - 2];
+#pragma unroll
+  for (int k = D - 3; k >= 0; --k) den = fmaf(x, den, c[O + N + k]);
+  den = fmaf(x, den, 1.0f);
+  return __fdividef(num, den);
+}
+
+// Fit evaluation policies.  c64 / c32 point at one reaction type's
+// coefficient pool (FP64 and FP32 copies).
+struct GenericFits {
+  const double* __restrict__ c64;
+  const float* __restrict__ c32;
+  const FitShape* sh;
+  template <int SLOT>
+  __device__ __forceinline__ double f64(double x) const
+  {
+    return fit_eval<double>(c64 + sh->offset[SLOT], sh->numer[SLOT], sh->denom[SLOT], x);
+  }
+  template <int SLOT>
+  __device__ __forceinline__ float fmix(float xf, double xd) const
+  {
+    if ((sh->fp64mask >> SLOT) & 1u) return (float)f64<SLOT>(xd);
+    return fit_eval_fast(c32 + sh->offset[SLOT], sh->numer[SLOT], sh->denom[SLOT], xf);
+  }
+};
+
+struct SpecFits {
+  const double* __restrict__ c64;
+  const float* __restrict__ c32;
+  template <int SLOT>
+  __device__ __forceinline__ double f64(double x) const { return fit_spec64<SLOT>(c64, x); }
+  template <int SLOT>
+  __device__ __forceinline__ float fmix(float xf, double xd) const
+  {
+    if ((kSpecFp64Mask >> SLOT) & 1u) return (float)fit_spec64<SLOT>(c64, xd);
+    return fit_spec32<SLOT>(c32, xf);
+  }
+};
+
+// The state vector of one cell: concentrations in double, the other 13 in Real.
 template <typename Real>
 struct CellState {
   double caSR, caI, caSS, kI, naI;
   Real rPrime, Xr1, Xr2, Xs, d, f, f2, fCass, h, j, m, r, s;
 };
 
+struct ConstsD {
+  static constexpr double Cm = 0.185, F = 96485.3415, R = 8314.472, T = 310;
+  static constexpr double Vc = 0.016404, Cao = 2, BufC = 0.2, BufSr = 10, BufSs = 0.4, EC = 1.5;
+  static constexpr double KbufC = 0.001, KbufSr = 0.3, KbufSs = 0.00025, Kup = 0.00025;
+  static constexpr double Vleak = 0.00036, Vrel = 0.102, Vsr = 0.001094, Vss = 5.468e-5;
+  static constexpr double Vxfer = 0.0038, VmaxUp = 0.006375, K1p = 0.15, K2p = 0.045, K3 = 0.06;
+  static constexpr double K4 = 0.005, MaxSr = 2.5, MinSr = 1, KpCa = 0.0005, KNaCa = 1000;
+  static constexpr double Ksat = 0.1, KmCa = 1.38, KmNai = 87.5, Alpha = 2.5, Ko = 5.4;
+  static constexpr double Pkna = 0.03, Nao = 140, KmNa = 40;
+};
+
 // FP64 step, the reference's expression order.
-__device__ __forceinline__ double tt06_step(const TT06Scalars& p, const BlockScale& blk,
-                                            const double* __restrict__ coef, const FitShape& sh,
+template <class Fits>
+__device__ __forceinline__ double tt06_step(const TT06Scalars& p, const BlockScale& blk, const Fits& fits,
                                             double dt, double V, CellState<double>& st)
 {
-  using C = Consts<double>;
-#define FIT(slot, x) fit_eval<double>(coef + sh.offset[slot], sh.numer[slot], sh.denom[slot], (x))
+  using C = ConstsD;
+#define FIT(slot, x) fits.template f64<slot>(x)
   const double gKr = p.g_Kr * (double)blk.g_Kr, gCaL = p.g_CaL * (double)blk.g_CaL, gNa = p.g_Na * (double)blk.g_Na;
   const double sqrtKo = 2.32379000772445;   // sqrt(5.4) in double
   const double RT = C::R * C::T;
@@ -203,13 +269,14 @@ __device__ __forceinline__ double tt06_step(const TT06Scalars& p, const BlockSca
   return -iIon;
 }
 
-// Mixed step: FP32 fits/gates/currents, FP64 concentration and R_prime
-// storage updates.  Returns dVm = -Iion in float.
-__device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const BlockScale& blk,
-                                                 const float* __restrict__ coef, const FitShape& sh,
-                                                 float dtf, double dt, double V, CellState<float>& st)
+// Mixed step.  Returns dVm = -Iion in float.
+template <class Fits>
+__device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const BlockScale& blk, const Fits& fits,
+                                                 float dtf, double V, CellState<float>& st)
 {
-#define FIT(slot, x) fit_eval_fast(coef + sh.offset[slot], sh.numer[slot], sh.denom[slot], (x))
+  // every V-fit takes V; its FP32 argument is Vf
+#define FIT(slot, x) fits.template fmix<slot>(x, V)
+#define FITX(slot, xf, xd) fits.template fmix<slot>(xf, xd)
   constexpr float Cm = 0.185f, F = 96485.3415f, RT = 8314.472f * 310.0f, Vc = 0.016404f, Cao = 2.0f;
   constexpr float BufC = 0.2f, BufSr = 10.0f, BufSs = 0.4f, EC2 = 1.5f * 1.5f;
   constexpr float KbufC = 0.001f, KbufSr = 0.3f, KbufSs = 0.00025f, Kup2 = 0.00025f * 0.00025f;
@@ -231,7 +298,7 @@ __device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const Blo
   const float ad = FIT(F_d_a, Vf), bd = FIT(F_d_b, Vf);
   const float af = FIT(F_f_a, Vf), bf = FIT(F_f_b, Vf);
   const float af2 = FIT(F_f2_a, Vf), bf2 = FIT(F_f2_b, Vf);
-  const float aFc = FIT(F_fCass_a, caSS), bFc = -fCassInf;
+  const float aFc = FITX(F_fCass_a, caSS, st.caSS), bFc = -fCassInf;
   const float ah = FIT(F_h_a, Vf), bh = FIT(F_h_b, Vf);
   const float aj = FIT(F_j_a, Vf), bj = FIT(F_j_b, Vf);
   const float am = FIT(F_m_a, Vf), bm = FIT(F_m_b, Vf);
@@ -267,7 +334,7 @@ __device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const Blo
   constexpr float naCaDen0 = (nao3 + kmnai3) * (Cao + KmCa);
   const float iNaCa = __fdividef(KNaCa * ((naI * naI * naI) * Cao * expG - nao3 * caI * Alpha * expGm1),
                                  naCaDen0 * (Ksat * expGm1 + 1.0f));
-  const float iK1 = FIT(F_K1, vEK);
+  const float iK1 = FITX(F_K1, vEK, V - (double)eK);
   const float iPK = vEK * (float)p.g_pK * pKterm;
   const float iKr = 0.430331482911935f * 2.3237900077f * vEK * st.Xr1 * st.Xr2 * gKr;
   const float eNa = RT_F * logf(__fdividef(Nao, naI));
@@ -306,8 +373,8 @@ __device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const Blo
   st.m += am * (st.m + bm);
   st.r += ar * (st.r + br);
   st.s += as * (st.s + bs);
-  (void)dt;
 #undef FIT
+#undef FITX
   return -iIon;
 }
 
