@@ -99,6 +99,8 @@ def load():
         "cdb_fgr_calc": (st, [vp, vp, vp]),
         "cdb_fgr_get_weights": (st, [vp, dp]),
         "cdb_fgr_destroy": (st, [vp]),
+        "cdb_fgr_calc_static": (st, [ctypes.c_int, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp, vp, vp,
+                                     ctypes.c_double, vp]),
         "cdb_engine_create": (st, [ctypes.POINTER(EngineConfig), vpp]),
         "cdb_engine_destroy": (st, [vp]),
         "cdb_engine_add_reaction": (st, [vp, ctypes.POINTER(TT06Params), ctypes.POINTER(Fit), i32p]),

@@ -129,6 +129,23 @@ cdb_status cdb_fgr_calc(cdb_fgr* d, double* dVm, void* stream);
 cdb_status cdb_fgr_get_weights(cdb_fgr* d, double* host19);
 cdb_status cdb_fgr_destroy(cdb_fgr* d);
 
+/* The FGR stencil for callers that cannot allocate device memory (code
+ * inside another framework's allocator, or measurement code that must leave
+ * the allocation state unchanged).  No counterpart in the reference.
+ * dVm[i] = diffusionScale (A0 phi0 + sum_k A_k phi_k) on a full nx*ny*nz box
+ * in gid order (x fastest); weights19 (device) is 19 rows of nCells doubles,
+ * row 0 = A0 and rows 1..18 = A[1..18] in NodeLocation order (the rows of
+ * cdb_fgr_get_weights, transposed); Vm and dVm are device arrays of nCells.
+ * The padded Vm block lives in a static device array of 16 MiB
+ * ((nx+2)(ny+2)(nz+2) <= 2,097,152 voxels, e.g. 126^3); larger boxes are
+ * rejected with CDB_INVALID_ARG.  The call allocates nothing: no cudaMalloc,
+ * no cudaFree.  Its first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  Every call shares the one array and clears it first; calls that
+ * overlap on the GPU (other streams, other threads) race on it. */
+cdb_status cdb_fgr_calc_static(int device, int32_t nx, int32_t ny, int32_t nz, const double* weights19,
+                               const double* Vm, double* dVm, double diffusionScale, void* stream);
+
 /* ------------------------------------------------------------------ */
 /* Fused engine                                                          */
 /* ------------------------------------------------------------------ */
