@@ -9,7 +9,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libcardioid_b200.so")
+# CARDIOID_B200_LIB names another build of the same library (e.g. one
+# compiled with different launch bounds); the default is the in-tree build.
+LIB_PATH = os.environ.get("CARDIOID_B200_LIB") or os.path.join(HERE, "_lib", "libcardioid_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "cardioid_b200.h")
 
 CDB_OK, CDB_INVALID_ARG, CDB_OOM, CDB_CUDA_ERROR, CDB_NUMERIC_FAULT, CDB_TIMEOUT, CDB_NOT_FOUND = range(7)

@@ -12,7 +12,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libcardioid_b200.so")
 SOURCES = ["engine_host.cu", "plugins.cu", "static_scratch.cu"]
-HEADERS = ["common.cuh", "tt06_device.cuh", "fgr_device.cuh", "step_kernel.cuh", "fit_shapes.h",
+HEADERS = ["common.cuh", "tt06_device.cuh", "tt06_step.cuh", "fgr_device.cuh", "step_kernel.cuh", "fit_shapes.h",
            os.path.join("..", "..", "include", "cardioid_b200.h")]
 
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--extended-lambda", "-gencode", "arch=compute_100a,code=sm_100a",

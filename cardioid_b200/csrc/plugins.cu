@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "fgr_device.cuh"
+#include "tt06_step.cuh"
 
 namespace cdb {
 
@@ -40,27 +41,13 @@ __global__ void __launch_bounds__(128) reaction_calc_kernel(ReactionArgs a, doub
   const double V = Vm[e];
   const BlockScale none{1.f, 1.f, 1.f};
   if (MIXED) {
-    double* s64 = a.s64 + i;
-    float* s32 = a.s32 + i;
-    CellState<float> st;
-    st.caSR = s64[0]; st.caI = s64[n]; st.caSS = s64[2 * n]; st.kI = s64[3 * n]; st.naI = s64[4 * n];
-    float* g = &st.rPrime;
-    // R_prime then the 12 gates, contiguous in CellState<float>
-    for (int k = 0; k < 13; ++k) g[k] = s32[k * n];
+    IOMixed io{a.s64 + i, a.s32 + i, n};
     GenericFits fits{a.coef64, a.coef32, &a.sh};
-    dVm[e] = (double)tt06_step_mixed(a.p, none, fits, (float)dt, V, st);
-    s64[0] = st.caSR; s64[n] = st.caI; s64[2 * n] = st.caSS; s64[3 * n] = st.kI; s64[4 * n] = st.naI;
-    for (int k = 0; k < 13; ++k) s32[k * n] = g[k];
+    dVm[e] = (double)tt06_step_mixed(a.p, none, fits, (float)dt, V, io);
   } else {
-    double* s = a.s64 + i;
-    CellState<double> st;
-    st.caSR = s[0]; st.caI = s[n]; st.caSS = s[2 * n]; st.kI = s[3 * n]; st.naI = s[4 * n];
-    double* g = &st.rPrime;
-    for (int k = 0; k < 13; ++k) g[k] = s[(5 + k) * n];
+    IO64 io{a.s64 + i, n};
     GenericFits fits{a.coef64, nullptr, &a.sh};
-    dVm[e] = tt06_step(a.p, none, fits, dt, V, st);
-    s[0] = st.caSR; s[n] = st.caI; s[2 * n] = st.caSS; s[3 * n] = st.kI; s[4 * n] = st.naI;
-    for (int k = 0; k < 13; ++k) s[(5 + k) * n] = g[k];
+    dVm[e] = tt06_step(a.p, none, fits, dt, V, io);
   }
 }
 

@@ -17,6 +17,7 @@
 
 #include "common.cuh"
 #include "fgr_device.cuh"
+#include "tt06_step.cuh"
 
 namespace cdb {
 
@@ -136,8 +137,18 @@ __device__ __forceinline__ double stencil32(const float* __restrict__ w, int64_t
   return (double)tmp;
 }
 
+// Resident CTAs per SM the register budget aims at: 4 CTAs (16 warps, 128
+// registers).  The mixed step fits without spilling; the FP64 step spills
+// ~90 bytes per thread to L1 there, and still runs 1.2x faster on B200 than
+// at 3 CTAs (168 registers, no spill) because latency hiding dominates.
+#ifndef CDB_FP64_MIN_CTAS
+#define CDB_FP64_MIN_CTAS 4
+#endif
+template <bool MIXED>
+constexpr int min_ctas() { return MIXED ? 4 : CDB_FP64_MIN_CTAS; }
+
 template <bool MIXED, bool SPEC>
-__global__ void __launch_bounds__(kCta) fused_step_kernel(StepArgs a)
+__global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(StepArgs a)
 {
   const int warp = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
   if (warp >= a.nTiles) return;   // whole warps leave together
@@ -205,41 +216,24 @@ __global__ void __launch_bounds__(kCta) fused_step_kernel(StepArgs a)
     const double* c64 = c_coef64 + rt * kFitPoolPerType;
     double dvmR;
     if (MIXED) {
-      CellState<float> st;
-      st.caSR = s64[0 * n]; st.caI = s64[1 * n]; st.caSS = s64[2 * n]; st.kI = s64[3 * n]; st.naI = s64[4 * n];
-      st.rPrime = s32[0 * n]; st.Xr1 = s32[1 * n]; st.Xr2 = s32[2 * n]; st.Xs = s32[3 * n]; st.d = s32[4 * n];
-      st.f = s32[5 * n]; st.f2 = s32[6 * n]; st.fCass = s32[7 * n]; st.h = s32[8 * n]; st.j = s32[9 * n];
-      st.m = s32[10 * n]; st.r = s32[11 * n]; st.s = s32[12 * n];
+      IOMixed io{s64, s32, n};
       const float* c32 = c_coef32 + rt * kFitPoolPerType;
       if (SPEC) {
         SpecFits fits{c64, c32};
-        dvmR = (double)tt06_step_mixed(c_scal[rt], blk, fits, (float)a.dt, phi0, st);
+        dvmR = (double)tt06_step_mixed(c_scal[rt], blk, fits, (float)a.dt, phi0, io);
       } else {
         GenericFits fits{c64, c32, &c_shape[rt]};
-        dvmR = (double)tt06_step_mixed(c_scal[rt], blk, fits, (float)a.dt, phi0, st);
+        dvmR = (double)tt06_step_mixed(c_scal[rt], blk, fits, (float)a.dt, phi0, io);
       }
-      s64[0 * n] = st.caSR; s64[1 * n] = st.caI; s64[2 * n] = st.caSS; s64[3 * n] = st.kI; s64[4 * n] = st.naI;
-      s32[0 * n] = st.rPrime; s32[1 * n] = st.Xr1; s32[2 * n] = st.Xr2; s32[3 * n] = st.Xs; s32[4 * n] = st.d;
-      s32[5 * n] = st.f; s32[6 * n] = st.f2; s32[7 * n] = st.fCass; s32[8 * n] = st.h; s32[9 * n] = st.j;
-      s32[10 * n] = st.m; s32[11 * n] = st.r; s32[12 * n] = st.s;
     } else {
-      CellState<double> st;
-      double* s = s64;
-      st.caSR = s[S_Ca_SR * n]; st.caI = s[S_Ca_i * n]; st.caSS = s[S_Ca_ss * n]; st.kI = s[S_K_i * n];
-      st.naI = s[S_Na_i * n]; st.rPrime = s[S_R_prime * n]; st.Xr1 = s[S_Xr1 * n]; st.Xr2 = s[S_Xr2 * n];
-      st.Xs = s[S_Xs * n]; st.d = s[S_d * n]; st.f = s[S_f * n]; st.f2 = s[S_f2 * n]; st.fCass = s[S_fCass * n];
-      st.h = s[S_h * n]; st.j = s[S_j * n]; st.m = s[S_m * n]; st.r = s[S_r * n]; st.s = s[S_s * n];
+      IO64 io{s64, n};
       if (SPEC) {
         SpecFits fits{c64, nullptr};
-        dvmR = tt06_step(c_scal[rt], blk, fits, a.dt, phi0, st);
+        dvmR = tt06_step(c_scal[rt], blk, fits, a.dt, phi0, io);
       } else {
         GenericFits fits{c64, nullptr, &c_shape[rt]};
-        dvmR = tt06_step(c_scal[rt], blk, fits, a.dt, phi0, st);
+        dvmR = tt06_step(c_scal[rt], blk, fits, a.dt, phi0, io);
       }
-      s[S_Ca_SR * n] = st.caSR; s[S_Ca_i * n] = st.caI; s[S_Ca_ss * n] = st.caSS; s[S_K_i * n] = st.kI;
-      s[S_Na_i * n] = st.naI; s[S_R_prime * n] = st.rPrime; s[S_Xr1 * n] = st.Xr1; s[S_Xr2 * n] = st.Xr2;
-      s[S_Xs * n] = st.Xs; s[S_d * n] = st.d; s[S_f * n] = st.f; s[S_f2 * n] = st.f2; s[S_fCass * n] = st.fCass;
-      s[S_h * n] = st.h; s[S_j * n] = st.j; s[S_m * n] = st.m; s[S_r * n] = st.r; s[S_s * n] = st.s;
     }
 
     vnew = phi0 + a.dt * (dvmR + dvmD + istim);
