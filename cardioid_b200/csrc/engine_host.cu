@@ -228,14 +228,9 @@ struct Engine {
         a.k = s;
         a.minmax = (minmax && s == k - 1) ? 1 : 0;
         const unsigned grid = grid_for(a.nTiles, kWarpsPerCta);
-        const bool sp = spec[st.first];
-        if (cfg.precision == CDB_MIXED) {
-          if (sp) fused_step_kernel<true, true><<<grid, kCta, 0, stream>>>(a);
-          else fused_step_kernel<true, false><<<grid, kCta, 0, stream>>>(a);
-        } else {
-          if (sp) fused_step_kernel<false, true><<<grid, kCta, 0, stream>>>(a);
-          else fused_step_kernel<false, false><<<grid, kCta, 0, stream>>>(a);
-        }
+        const int slot = spec[st.first] ? st.first : -1;
+        if (cfg.precision == CDB_MIXED) launch_step<true>(slot, grid, stream, a);
+        else launch_step<false>(slot, grid, stream, a);
         ++launches;
       }
     }

@@ -346,3 +346,24 @@ cdb_status cdb_fgr_destroy(cdb_fgr* d)
 }
 
 }  // extern "C"
+
+// ---- diagnostics ----
+
+namespace cdb {
+__global__ void diag_div64_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                                  double* __restrict__ q)
+{
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) q[i] = div64(a[i], b[i]);
+}
+}  // namespace cdb
+
+extern "C" cdb_status cdb_diag_div64(int device, int64_t n, const double* a, const double* b, double* q, void* stream)
+{
+  CDB_CHECK(a && b && q && n >= 0, CDB_INVALID_ARG, "bad argument");
+  CDB_CUDA(cudaSetDevice(device));
+  if (n == 0) return CDB_OK;
+  diag_div64_kernel<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(n, a, b, q);
+  CDB_CUDA(cudaGetLastError());
+  return CDB_OK;
+}

@@ -147,9 +147,13 @@ __device__ __forceinline__ double stencil32(const float* __restrict__ w, int64_t
 template <bool MIXED>
 constexpr int min_ctas() { return MIXED ? 4 : CDB_FP64_MIN_CTAS; }
 
-template <bool MIXED, bool SPEC>
+// SLOT >= 0: the launch's reaction type is constant-memory slot SLOT and its
+// fits have the compiled shapes (fit_shapes.h); SLOT < 0: any slot (a.rt)
+// with run-time shapes.
+template <bool MIXED, int SLOT>
 __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(StepArgs a)
 {
+  constexpr bool SPEC = SLOT >= 0;
   const int warp = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
   if (warp >= a.nTiles) return;   // whole warps leave together
   const int lane = threadIdx.x & 31;
@@ -212,7 +216,9 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
       dvmD = acc * scale;
     }
 
-    const int rt = a.rt;
+    // With SPEC the slot is a template parameter, so every coefficient is
+    // an immediate constant-bank operand of its FMA (no load instruction).
+    const int rt = SPEC ? SLOT : a.rt;
     const double* c64 = c_coef64 + rt * kFitPoolPerType;
     double dvmR;
     if (MIXED) {
@@ -254,6 +260,23 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
       atomicMin(Tp->minmax, ordered_bits(lo));
       atomicMax(Tp->minmax + 1, ordered_bits(hi));
     }
+  }
+}
+
+// One step of one reaction type: the compiled kernel of its slot when the
+// type has the compiled fit shapes (slot >= 0), else the generic kernel.
+template <bool MIXED>
+inline void launch_step(int slot, unsigned grid, cudaStream_t stream, const StepArgs& a)
+{
+  static_assert(CDB_MAX_REACTION_TYPES == 6, "one compiled kernel per slot");
+  switch (slot) {
+    case 0: fused_step_kernel<MIXED, 0><<<grid, kCta, 0, stream>>>(a); break;
+    case 1: fused_step_kernel<MIXED, 1><<<grid, kCta, 0, stream>>>(a); break;
+    case 2: fused_step_kernel<MIXED, 2><<<grid, kCta, 0, stream>>>(a); break;
+    case 3: fused_step_kernel<MIXED, 3><<<grid, kCta, 0, stream>>>(a); break;
+    case 4: fused_step_kernel<MIXED, 4><<<grid, kCta, 0, stream>>>(a); break;
+    case 5: fused_step_kernel<MIXED, 5><<<grid, kCta, 0, stream>>>(a); break;
+    default: fused_step_kernel<MIXED, -1><<<grid, kCta, 0, stream>>>(a); break;
   }
 }
 

@@ -64,6 +64,39 @@ struct BlockScale {
   float g_Kr, g_CaL, g_Na;
 };
 
+// FP64 quotient without the slow-path branch of the IEEE division: the
+// hardware reciprocal approximation (PTX rcp.approx.ftz.f64) refined by two
+// Newton-Raphson steps r <- r + r (1 - b r), then the quotient corrected
+// once by its residual, q <- q + r (a - b q) (Markstein's method, IBM J.
+// Res. Dev. 34(1), 1990).  Within a few ulp of a / b for the normal,
+// finite operands of the model (tests/test_division_gpu.py measures it
+// against CUDA's a / b); subnormal divisors flush to zero.  Defining
+// CDB_IEEE_DIV restores a / b.
+__device__ __forceinline__ double rcp64(double b)
+{
+#ifdef CDB_IEEE_DIV
+  return 1.0 / b;
+#else
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+  double e = fma(-b, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-b, r, 1.0);
+  return fma(r, e, r);
+#endif
+}
+
+__device__ __forceinline__ double div64(double a, double b)
+{
+#ifdef CDB_IEEE_DIV
+  return a / b;
+#else
+  const double r = rcp64(b);
+  const double q = a * r;
+  return fma(r, fma(-b, q, a), q);
+#endif
+}
+
 // Horner numerator over (1 + x * Horner denominator); the monomial form
 // of the FIT files (elec/Interpolation.hh:11-99).
 template <typename Real>
@@ -108,7 +141,7 @@ __device__ __forceinline__ double fit_spec64(const double* __restrict__ c, doubl
 #pragma unroll
   for (int k = D - 3; k >= 0; --k) den = c[O + N + k] + x * den;
   den = 1.0 + x * den;
-  return num / den;
+  return div64(num, den);
 }
 
 template <int SLOT>
@@ -167,6 +200,9 @@ struct ConstsD {
   static constexpr double K4 = 0.005, MaxSr = 2.5, MinSr = 1, KpCa = 0.0005, KNaCa = 1000;
   static constexpr double Ksat = 0.1, KmCa = 1.38, KmNai = 87.5, Alpha = 2.5, Ko = 5.4;
   static constexpr double Pkna = 0.03, Nao = 140, KmNa = 40;
+  // reciprocals of the constant divisors (x / c becomes x * (1/c))
+  static constexpr double InvF = 1.0 / F, InvFVc = 1.0 / (F * Vc), InvVc = 1.0 / Vc;
+  static constexpr double InvFVss = 1.0 / (F * Vss), InvVss = 1.0 / Vss;
 };
 
 }  // namespace cdb

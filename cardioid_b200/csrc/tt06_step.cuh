@@ -5,9 +5,10 @@
 // gate values, V and seven fits), the concentrations and R_prime stored as
 // soon as they are known, then each gate's two Rush-Larsen fits, its update
 // and its store, one gate at a time.  Only independent work moves relative
-// to the reference's listing, so every value is computed by the same
-// operations; the short live ranges keep the register count (and with it the
-// number of resident warps) in check.
+// to the reference's listing; the short live ranges keep the register count
+// (and with it the number of resident warps) in check.  In the FP64 step a
+// division by a model constant is a product with its reciprocal and every
+// other division is div64 (branch-free), which moves results by a few ulp.
 //
 // IO policy: get<k>() loads state k (checkpoint order), put<k>(v) stores it.
 #pragma once
@@ -34,48 +35,50 @@ __device__ __forceinline__ double tt06_step(const TT06Scalars& p, const BlockSca
   const double m = io.template get<S_m>(), r = io.template get<S_r>(), s = io.template get<S_s>();
 
   // currents
+  // (divisions by constants are products with their reciprocals; the rest
+  // go through div64, so no division takes a branch)
   const double calT3 = FIT(F_CalT3, V), calT4 = FIT(F_CalT4, V);
-  const double eCa = 0.5 * C::R * C::T * log(C::Cao / caI) / C::F;
+  const double eCa = 0.5 * C::R * C::T * log(div64(C::Cao, caI)) * C::InvF;
   const double iBCa = p.g_bca * (V - eCa);
-  const double iPCa = caI * p.g_pCa / (caI + C::KpCa);
+  const double iPCa = div64(caI * p.g_pCa, caI + C::KpCa);
   const double expG = FIT(F_expG, V), expGm1 = FIT(F_expGm1, V);
   const double pKterm = FIT(F_pKterm, V);
-  const double eK = RT * log(C::Ko / kI) / C::F;
+  const double eK = RT * log(div64(C::Ko, kI)) * C::InvF;
   const double naKterm = FIT(F_NaKterm, V);
-  const double iNaK = naI * naKterm / (naI + C::KmNa);
+  const double iNaK = div64(naI * naKterm, naI + C::KmNa);
   const double vEK = -eK + V;
-  const double bufC = 1.0 / (C::BufC * C::KbufC / ((caI + C::KbufC) * (caI + C::KbufC)) + 1);
-  const double bufSR = 1.0 / (C::BufSr * C::KbufSr / ((caSR + C::KbufSr) * (caSR + C::KbufSr)) + 1);
-  const double bufSS = 1.0 / (C::BufSs * C::KbufSs / ((caSS + C::KbufSs) * (caSS + C::KbufSs)) + 1);
+  const double bufC = rcp64(div64(C::BufC * C::KbufC, (caI + C::KbufC) * (caI + C::KbufC)) + 1);
+  const double bufSR = rcp64(div64(C::BufSr * C::KbufSr, (caSR + C::KbufSr) * (caSR + C::KbufSr)) + 1);
+  const double bufSS = rcp64(div64(C::BufSs * C::KbufSs, (caSS + C::KbufSs) * (caSS + C::KbufSs)) + 1);
   const double iLeak = C::Vleak * (caSR - caI);
-  const double iUp = C::VmaxUp / (1 + (C::Kup * C::Kup) / (caI * caI));
+  const double iUp = div64(C::VmaxUp, 1 + div64(C::Kup * C::Kup, caI * caI));
   const double iXfer = C::Vxfer * (-caI + caSS);
-  const double kcasr = C::MaxSr - (C::MaxSr - C::MinSr) / (1 + (C::EC * C::EC) / (caSR * caSR));
-  const double k1 = C::K1p / kcasr, k2 = C::K2p * kcasr;
-  const double O = (caSS * caSS) * rPrime * k1 / ((caSS * caSS) * k1 + C::K3);
+  const double kcasr = C::MaxSr - div64(C::MaxSr - C::MinSr, 1 + div64(C::EC * C::EC, caSR * caSR));
+  const double k1 = div64(C::K1p, kcasr), k2 = C::K2p * kcasr;
+  const double O = div64((caSS * caSS) * rPrime * k1, (caSS * caSS) * k1 + C::K3);
   const double dRprime = -caSS * rPrime * k2 + C::K4 * (-rPrime + 1);
   const double iRel = O * C::Vrel * (caSR - caSS);
   const double dCaSR = bufSR * (-iLeak - iRel + iUp);
   const double iCaL = d * f * f2 * fCass * gCaL * (-C::Cao * calT3 + 0.25 * caSS * calT4);
   const double nao3 = C::Nao * C::Nao * C::Nao, kmnai3 = C::KmNai * C::KmNai * C::KmNai;
-  const double iNaCa = C::KNaCa * ((naI * naI * naI) * C::Cao * expG - nao3 * caI * C::Alpha * expGm1) /
-                       ((nao3 + kmnai3) * (C::Cao + C::KmCa) * (C::Ksat * expGm1 + 1));
+  const double iNaCa = div64(C::KNaCa * ((naI * naI * naI) * C::Cao * expG - nao3 * caI * C::Alpha * expGm1),
+                             (nao3 + kmnai3) * (C::Cao + C::KmCa) * (C::Ksat * expGm1 + 1));
   const double iK1 = FIT(F_K1, vEK);
   const double iPK = vEK * p.g_pK * pKterm;
   const double iKr = 0.430331482911935 * vEK * sqrtKo * Xr1 * Xr2 * gKr;
-  const double eNa = RT * log(C::Nao / naI) / C::F;
-  const double eKs = RT * log((C::Ko + C::Nao * C::Pkna) / (kI + naI * C::Pkna)) / C::F;
+  const double eNa = RT * log(div64(C::Nao, naI)) * C::InvF;
+  const double eKs = RT * log(div64(C::Ko + C::Nao * C::Pkna, kI + naI * C::Pkna)) * C::InvF;
   const double iKs = (Xs * Xs) * p.g_Ks * (V - eKs);
   const double iBNa = p.g_bna * (-eNa + V);
   const double iTo = vEK * p.g_to * r * s;
   const double kTot = -2 * iNaK + iK1 + iPK + iKr + iKs + iTo;
   const double halfCm = -0.5 * C::Cm;
-  const double dCaI = bufC * (halfCm * (-2 * iNaCa + iBCa + iPCa) / (C::F * C::Vc) + iXfer + C::Vsr * (iLeak - iUp) / C::Vc);
-  const double dCaSS = bufSS * (halfCm * iCaL / (C::F * C::Vss) - C::Vc * iXfer / C::Vss + C::Vsr * iRel / C::Vss);
+  const double dCaI = bufC * (halfCm * (-2 * iNaCa + iBCa + iPCa) * C::InvFVc + iXfer + C::Vsr * (iLeak - iUp) * C::InvVc);
+  const double dCaSS = bufSS * (halfCm * iCaL * C::InvFVss - C::Vc * iXfer * C::InvVss + C::Vsr * iRel * C::InvVss);
   const double iNa = (m * m * m) * gNa * h * j * (-eNa + V);
-  const double dKi = -C::Cm * kTot / (C::F * C::Vc);
+  const double dKi = -C::Cm * kTot * C::InvFVc;
   const double naTot = iNa + 3 * iNaK + iBNa + 3 * iNaCa;
-  const double dNai = -C::Cm * naTot / (C::F * C::Vc);
+  const double dNai = -C::Cm * naTot * C::InvFVc;
   const double caTot = iCaL + iPCa + iBCa + -2 * iNaCa;
   const double iIon = caTot + kTot + naTot;
 
@@ -100,7 +103,7 @@ __device__ __forceinline__ double tt06_step(const TT06Scalars& p, const BlockSca
   GATE(S_f, f, F_f_a, F_f_b, V)
   GATE(S_f2, f2, F_f2_a, F_f2_b, V)
   {
-    const double fCassInf = 0.4 + 0.6 / (400.0 * (caSS * caSS) + 1);
+    const double fCassInf = 0.4 + div64(0.6, 400.0 * (caSS * caSS) + 1);
     const double ga = FIT(F_fCass_a, caSS), gb = -fCassInf;
     io.template put<S_fCass>(fCass + ga * (fCass + gb));
   }

@@ -209,6 +209,14 @@ cdb_status cdb_engine_read_weights(cdb_engine* e, int32_t id, double* host19);
  * own state; this is the per-step cost a caller that owns Vm on the host
  * pays. */
 cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, double* vm_out);
+/* ------------------------------------------------------------------ */
+/* Diagnostics                                                           */
+/* ------------------------------------------------------------------ */
+/* q[i] = a[i] / b[i] (device arrays) computed with the engine's branch-free
+ * FP64 quotient (Newton-refined reciprocal with a residual correction), for
+ * measuring it against IEEE division.  No counterpart in the reference. */
+cdb_status cdb_diag_div64(int device, int64_t n, const double* a, const double* b, double* q, void* stream);
+
 /* Kernels launched by this engine since creation. */
 cdb_status cdb_engine_launch_count(cdb_engine* e, int64_t* launches);
 /* The CUDA stream (cudaStream_t) the engine launches on. */
