@@ -122,6 +122,8 @@ def load():
         "cdb_engine_read_weights": (st, [vp, ctypes.c_int32, dp]),
         "cdb_engine_step_host": (st, [vp, ctypes.c_int32, dp, dp]),
         "cdb_engine_launch_count": (st, [vp, i64p]),
+        "cdb_engine_set_tuning": (st, [vp, ctypes.c_int32, ctypes.c_int32]),
+        "cdb_engine_get_tuning": (st, [vp, i32p, i32p]),
         "cdb_diag_div64": (st, [ctypes.c_int, ctypes.c_int64, vp, vp, vp, vp]),
         "cdb_engine_stream": (st, [vp, vpp]),
     }

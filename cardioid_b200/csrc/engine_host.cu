@@ -120,6 +120,10 @@ struct Engine {
   cudaGraphExec_t graph = nullptr;
   int graphSteps = 0;
   bool graphMinmax = false;
+  // launch tuning (cdb_engine_set_tuning; the autotuner picks them)
+  int stage = 1;           // 1: stage each warp's next tile through shared memory (cp.async)
+  int ctasPerSm = 4;       // persistent grid: SMs x this
+  int numSms = 148;
 
   ~Engine()
   {
@@ -169,7 +173,9 @@ struct Engine {
       while (f < t.n) {
         const uint8_t slot = t.slotOf[f];
         int64_t e = f + 1;
-        while (e < t.n && e - f < 32 && t.slotOf[e] == slot) ++e;
+        // a tile never crosses a 32-cell AoSoA block
+        const int64_t blockEnd = (f / kBlk + 1) * kBlk;
+        while (e < t.n && e < blockEnd && t.slotOf[e] == slot) ++e;
         WarpTile tl;
         tl.tissue = idx;
         tl.first = f;
@@ -227,7 +233,9 @@ struct Engine {
         a.dt = cfg.dt;
         a.k = s;
         a.minmax = (minmax && s == k - 1) ? 1 : 0;
-        const unsigned grid = grid_for(a.nTiles, kWarpsPerCta);
+        a.stage = stage;
+        const unsigned grid = (unsigned)std::min<int64_t>(grid_for(a.nTiles, kWarpsPerCta),
+                                                          (int64_t)numSms * ctasPerSm);
         const int slot = spec[st.first] ? st.first : -1;
         if (cfg.precision == CDB_MIXED) launch_step<true>(slot, grid, stream, a);
         else launch_step<false>(slot, grid, stream, a);
@@ -345,11 +353,12 @@ int64_t tissue_bytes(const Engine& E, const cdb_tissue_desc* t)
   const int cls = tissue_class(t->nx, t->ny, t->nz, masked);
   const int64_t vox = padded_voxels(t->nx, t->ny, t->nz, cls, nullptr, nullptr, nullptr, nullptr);
   const int64_t n = t->nCells;
+  const int64_t nPad = (n + kBlk - 1) / kBlk * kBlk;
   const bool mixed = E.cfg.precision == CDB_MIXED;
-  int64_t b = 2 * vox * 8;                                   // Vm blocks
-  b += mixed ? n * (5 * 8 + 13 * 4) : n * 18 * 8;           // state
-  b += mixed ? n * (class_rows(cls) - 1) * 4 : n * class_rows(cls) * 8;   // weights
-  b += n * 8 + (masked ? n * 8 : 0) + 64;                   // act, voxel
+  int64_t b = 2 * vox * 8;                                                   // Vm blocks
+  b += mixed ? nPad * (kRowsMixed64 * 8 + kRowsMixed32 * 4) : nPad * kRows64 * 8;   // state
+  b += nPad * weight_rows(cls, mixed) * (mixed ? 4 : 8);                     // weights
+  b += n * 8 + (masked ? n * 8 : 0) + 64;                                   // act, voxel
   return b;
 }
 
@@ -385,7 +394,33 @@ cdb_status cdb_engine_create(const cdb_engine_config* cfg, cdb_engine** out)
   std::unique_ptr<cdb_engine> e(new cdb_engine);
   e->e.cfg = *cfg;
   CDB_CUDA(cudaStreamCreateWithFlags(&e->e.stream, cudaStreamNonBlocking));
+  CDB_CUDA(cudaDeviceGetAttribute(&e->e.numSms, cudaDevAttrMultiProcessorCount, cfg->device));
   *out = e.release();
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_set_tuning(cdb_engine* e, int32_t stage, int32_t ctasPerSm)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  CDB_CHECK(stage == 0 || stage == 1, CDB_INVALID_ARG, "stage must be 0 or 1");
+  CDB_CHECK(ctasPerSm >= 1 && ctasPerSm <= 64, CDB_INVALID_ARG, "ctasPerSm must be in [1, 64]");
+  Engine& E = e->e;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  E.stage = stage;
+  E.ctasPerSm = ctasPerSm;
+  if (E.graph) {
+    cudaGraphExecDestroy(E.graph);
+    E.graph = nullptr;
+  }
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_get_tuning(cdb_engine* e, int32_t* stage, int32_t* ctasPerSm)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  if (stage) *stage = e->e.stage;
+  if (ctasPerSm) *ctasPerSm = e->e.ctasPerSm;
   return CDB_OK;
 }
 
@@ -479,14 +514,17 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
   CDB_CUDA(h->vm1.alloc(vox * 8));
   CDB_CUDA(cudaMemsetAsync(h->vm0.p, 0, vox * 8, s));
   CDB_CUDA(cudaMemsetAsync(h->vm1.p, 0, vox * 8, s));
+  // AoSoA arrays cover whole 32-cell blocks
+  const int64_t nPad = (n + kBlk - 1) / kBlk * kBlk;
   if (mixed) {
-    CDB_CUDA(h->s64.alloc(n * 5 * 8));
-    CDB_CUDA(h->s32.alloc(n * 13 * 4));
+    CDB_CUDA(h->s64.alloc(nPad * kRowsMixed64 * 8));
+    CDB_CUDA(h->s32.alloc(nPad * kRowsMixed32 * 4));
   } else {
-    CDB_CUDA(h->s64.alloc(n * 18 * 8));
+    CDB_CUDA(h->s64.alloc(nPad * kRows64 * 8));
   }
-  const int rows = class_rows(cls);
-  CDB_CUDA(h->w.alloc(mixed ? n * (rows - 1) * 4 : n * rows * 8));
+  const int wrows = weight_rows(cls, mixed);
+  CDB_CUDA(h->w.alloc(nPad * wrows * (mixed ? 4 : 8)));
+  CDB_CUDA(cudaMemsetAsync(h->w.p, 0, nPad * wrows * (mixed ? 4 : 8), s));
   CDB_CUDA(h->act.alloc(n * 8));
   CDB_CUDA(h->minmax.alloc(16));
   if (masked) CDB_CUDA(h->voxel.alloc(n * 8));
@@ -536,7 +574,7 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
   d.voxel = masked ? h->voxel.as<int64_t>() : nullptr;
   d.act = h->act.as<double>();
   d.minmax = h->minmax.as<unsigned long long>();
-  init_state_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, d.s64, d.s32, mixed ? 1 : 0, d.act);
+  init_state_kernel<<<grid_for(nPad, 256), 256, 0, s>>>(nPad, d.s64, d.s32, mixed ? 1 : 0, d.act, n);
   E.launches += 1;
   {
     DeviceBuffer v0;
@@ -647,13 +685,13 @@ cdb_status cdb_engine_read_state(cdb_engine* e, int32_t id, int var, double* hos
   CDB_CUDA(cudaSetDevice(E.cfg.device));
   CDB_CUDA(cudaStreamSynchronize(E.stream));
   const int64_t n = t->n;
-  if (E.cfg.precision == CDB_MIXED && var >= 5) {
-    std::vector<float> tmp(n);
-    CDB_CUDA(cudaMemcpy(tmp.data(), t->dev.s32 + (var - 5) * n, n * 4, cudaMemcpyDeviceToHost));
-    for (int64_t i = 0; i < n; ++i) host[i] = tmp[i];
-  } else {
-    CDB_CUDA(cudaMemcpy(host, t->dev.s64 + var * n, n * 8, cudaMemcpyDeviceToHost));
-  }
+  DeviceBuffer tmp;
+  CDB_CUDA(tmp.alloc(n * 8));
+  gather_state_kernel<<<grid_for(n, 256), 256, 0, E.stream>>>(n, t->dev.s64, t->dev.s32,
+                                                              E.cfg.precision == CDB_MIXED, var, tmp.as<double>());
+  E.launches += 1;
+  CDB_CUDA(cudaMemcpyAsync(host, tmp.p, n * 8, cudaMemcpyDeviceToHost, E.stream));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
   return CDB_OK;
 }
 
@@ -667,13 +705,13 @@ cdb_status cdb_engine_write_state(cdb_engine* e, int32_t id, int var, const doub
   CDB_CUDA(cudaSetDevice(E.cfg.device));
   CDB_CUDA(cudaStreamSynchronize(E.stream));
   const int64_t n = t->n;
-  if (E.cfg.precision == CDB_MIXED && var >= 5) {
-    std::vector<float> tmp(n);
-    for (int64_t i = 0; i < n; ++i) tmp[i] = (float)host[i];
-    CDB_CUDA(cudaMemcpy(t->dev.s32 + (var - 5) * n, tmp.data(), n * 4, cudaMemcpyHostToDevice));
-  } else {
-    CDB_CUDA(cudaMemcpy(t->dev.s64 + var * n, host, n * 8, cudaMemcpyHostToDevice));
-  }
+  DeviceBuffer tmp;
+  CDB_CUDA(tmp.alloc(n * 8));
+  CDB_CUDA(cudaMemcpyAsync(tmp.p, host, n * 8, cudaMemcpyHostToDevice, E.stream));
+  scatter_state_kernel<<<grid_for(n, 256), 256, 0, E.stream>>>(n, t->dev.s64, t->dev.s32,
+                                                               E.cfg.precision == CDB_MIXED, var, tmp.as<double>());
+  E.launches += 1;
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
   return CDB_OK;
 }
 
@@ -717,22 +755,24 @@ cdb_status cdb_engine_read_weights(cdb_engine* e, int32_t id, double* host19)
   const int rows = class_rows(cls);
   const bool mixed = E.cfg.precision == CDB_MIXED;
   std::vector<double> out(n * 19, 0.0);
+  const int64_t nPad = (n + kBlk - 1) / kBlk * kBlk;
   if (mixed) {
-    std::vector<float> w((size_t)n * (rows - 1));
+    std::vector<float> w((size_t)nPad * (rows - 1));
     CDB_CUDA(cudaMemcpy(w.data(), t->dev.w, w.size() * 4, cudaMemcpyDeviceToHost));
     for (int64_t i = 0; i < n; ++i) {
       double a0 = 0;
       for (int r = 1; r < rows; ++r) {
-        out[i * 19 + class_node(cls, r)] = w[(r - 1) * n + i];
-        a0 -= w[(r - 1) * n + i];
+        const float v = w[aosoa(i, rows - 1, r - 1)];
+        out[i * 19 + class_node(cls, r)] = v;
+        a0 -= v;
       }
       out[i * 19] = a0;
     }
   } else {
-    std::vector<double> w((size_t)n * rows);
+    std::vector<double> w((size_t)nPad * rows);
     CDB_CUDA(cudaMemcpy(w.data(), t->dev.w, w.size() * 8, cudaMemcpyDeviceToHost));
     for (int64_t i = 0; i < n; ++i)
-      for (int r = 0; r < rows; ++r) out[i * 19 + class_node(cls, r)] = w[r * n + i];
+      for (int r = 0; r < rows; ++r) out[i * 19 + class_node(cls, r)] = w[aosoa(i, rows, r)];
   }
   std::memcpy(host19, out.data(), out.size() * 8);
   return CDB_OK;

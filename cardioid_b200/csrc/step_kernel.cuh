@@ -1,10 +1,10 @@
 // The fused time-step kernel and its set-up kernels.
 //
-// One launch per (time step, reaction type present): each warp takes one
-// warp tile, a run of up to 32 consecutive cells of one tissue that share a
-// reaction type, so the type — and with it the coefficient pool — is a
-// kernel parameter, uniform across the launch.  Per cell, in the order of
-// the reference's omp loop (elec/simulationLoop.cc:183-231):
+// One launch per (time step, reaction type present): each warp takes warp
+// tiles, runs of up to 32 consecutive cells of one tissue that share a
+// reaction type and lie in one 32-cell block, so the type — and with it the
+// coefficient pool — is a kernel parameter, uniform across the launch.  Per
+// cell, in the order of the reference's omp loop (elec/simulationLoop.cc:183-231):
 //   FGR stencil on Vm(t) (elec/FGRDiffusionOMP.cc:109-131),
 //   BetterTT06 update (elec/BetterTT06.cc:1426-1649),
 //   box stimuli, assigned in order (elec/BoxStimulus.cc:56-64),
@@ -12,6 +12,14 @@
 //   activation time: first post-step time with Vm > 0 (elec/ActivationTimeSensor.cc:99-111),
 //   min/max Vm (elec/MinMaxSensor.cc:44-67) on request.
 // Vm is read from one padded block and written to the other.
+//
+// State and weights are stored in AoSoA blocks of 32 cells (block b holds
+// row r of its 32 cells contiguously at [b][r][0..31]), so a tile's inputs
+// are a few contiguous, 16-byte-aligned runs.  The kernel is persistent over
+// its tiles: while a warp computes one tile it has the next tile's state
+// block (and, for the mixed path, weight block) copied into shared memory
+// with cp.async (double buffering), so the DRAM latency of those loads
+// overlaps the reaction's arithmetic.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -23,12 +31,13 @@ namespace cdb {
 
 constexpr int kWarpsPerCta = 4;
 constexpr int kCta = 32 * kWarpsPerCta;
+constexpr int kBlk = 32;   // cells per AoSoA block
 
 struct TissueDev {
   double* vm[2];
-  double* s64;
-  float* s32;
-  const void* w;
+  double* s64;            // AoSoA: FP64 [nb][18][32]; mixed [nb][5][32]
+  float* s32;             // AoSoA: mixed [nb][13][32]
+  const void* w;          // AoSoA: FP64 [nb][rows][32] doubles; mixed [nb][rows-1][32] floats
   const int64_t* voxel;
   double* act;
   int64_t n;
@@ -60,12 +69,27 @@ struct StepArgs {
   double dt;
   int k;                      // step within the launch batch
   int minmax;                 // reduce min/max this step
+  int stage;                  // 1: stage the next tile through shared memory
 };
 
 __constant__ TT06Scalars c_scal[CDB_MAX_REACTION_TYPES];
 __constant__ FitShape c_shape[CDB_MAX_REACTION_TYPES];
 __constant__ double c_coef64[CDB_MAX_REACTION_TYPES * kFitPoolPerType];
 __constant__ float c_coef32[CDB_MAX_REACTION_TYPES * kFitPoolPerType];
+
+// AoSoA row sizes
+constexpr int kRows64 = kNumStates;                 // FP64 state rows
+constexpr int kRowsMixed64 = 5, kRowsMixed32 = 13;  // mixed state rows
+__host__ __device__ constexpr int weight_rows(int cls, bool mixed) { return mixed ? class_rows(cls) - 1 : class_rows(cls); }
+
+// Shared-memory staging per warp and buffer: the mixed path stages its state
+// block and its weight block (up to 18 float rows), the FP64 path its state
+// block (its weights are read directly).
+template <bool MIXED>
+__host__ __device__ constexpr int stage_bytes()
+{
+  return MIXED ? (kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4 + 18 * kBlk * 4) : kRows64 * kBlk * 8;
+}
 
 __device__ __forceinline__ double pulse_value(const cdb_stimulus& s, double time)
 {
@@ -107,57 +131,107 @@ __device__ __forceinline__ int64_t node_offset(int64_t px, int64_t pxy, int node
   return (int64_t)node_dx(node) + px * node_dy(node) + pxy * node_dz(node);
 }
 
-// FP64 stencil in the reference's order: A0 phi0 + sum_k A_k phi_k.
+// FP64 stencil in the reference's order: A0 phi0 + sum_k A_k phi_k; w points
+// at the cell's row-0 weight, rows kBlk apart.
 template <int CLS>
-__device__ __forceinline__ double stencil64(const double* __restrict__ w, int64_t n, int64_t px, int64_t pxy,
-                                            const double* __restrict__ vin, int64_t vox, double phi0, int64_t i)
+__device__ __forceinline__ double stencil64(const double* __restrict__ w, int64_t px, int64_t pxy,
+                                            const double* __restrict__ vin, int64_t vox, double phi0)
 {
-  double tmp = __ldg(w + i) * phi0;
+  double tmp = __ldg(w) * phi0;
 #pragma unroll
   for (int r = 1; r < class_rows(CLS); ++r) {
     const int node = class_node(CLS, r);
-    tmp += __ldg(w + r * n + i) * __ldg(vin + vox + node_offset(px, pxy, node));
+    tmp += __ldg(w + r * kBlk) * __ldg(vin + vox + node_offset(px, pxy, node));
   }
   return tmp;
 }
 
-// Mixed stencil: sum_k A_k (phi_k - phi0) with FP32 weights; the
-// differences are taken in FP64 (A0 = -sum A_k).
+// Mixed stencil: sum_k A_k (phi_k - phi0) with FP32 weights (from shared
+// memory); the differences are taken in FP64 (A0 = -sum A_k).
 template <int CLS>
-__device__ __forceinline__ double stencil32(const float* __restrict__ w, int64_t n, int64_t px, int64_t pxy,
-                                            const double* __restrict__ vin, int64_t vox, double phi0, int64_t i)
+__device__ __forceinline__ double stencil32(const float* __restrict__ w, int64_t px, int64_t pxy,
+                                            const double* __restrict__ vin, int64_t vox, double phi0)
 {
   float tmp = 0.f;
 #pragma unroll
   for (int r = 1; r < class_rows(CLS); ++r) {
     const int node = class_node(CLS, r);
     const float d = (float)(__ldg(vin + vox + node_offset(px, pxy, node)) - phi0);
-    tmp = fmaf(__ldg(w + (r - 1) * n + i), d, tmp);
+    tmp = fmaf(w[(r - 1) * kBlk], d, tmp);
   }
   return (double)tmp;
 }
 
-// Resident CTAs per SM the register budget aims at: 4 CTAs (16 warps, 128
-// registers).  The mixed step fits without spilling; the FP64 step spills
-// ~90 bytes per thread to L1 there, and still runs 1.2x faster on B200 than
-// at 3 CTAs (168 registers, no spill) because latency hiding dominates.
-#ifndef CDB_FP64_MIN_CTAS
-#define CDB_FP64_MIN_CTAS 4
-#endif
-template <bool MIXED>
-constexpr int min_ctas() { return MIXED ? 4 : CDB_FP64_MIN_CTAS; }
+// State access of one cell in an AoSoA block: reads from the staged copy,
+// writes to the global block.
+struct IOBlock64 {
+  const double* __restrict__ src;   // [18][32], at the cell's column
+  double* __restrict__ dst;
+  template <int K> __device__ __forceinline__ double get() const { return src[K * kBlk]; }
+  template <int K> __device__ __forceinline__ void put(double v) const { dst[K * kBlk] = v; }
+};
 
-// SLOT >= 0: the launch's reaction type is constant-memory slot SLOT and its
-// fits have the compiled shapes (fit_shapes.h); SLOT < 0: any slot (a.rt)
-// with run-time shapes.
+struct IOBlockMixed {
+  const double* __restrict__ src64;   // [5][32]
+  const float* __restrict__ src32;    // [13][32]
+  double* __restrict__ dst64;
+  float* __restrict__ dst32;
+  template <int K> __device__ __forceinline__ double get() const
+  {
+    if (K < 5) return src64[K * kBlk];
+    return (double)src32[(K - 5) * kBlk];
+  }
+  template <int K> __device__ __forceinline__ void put(double v) const
+  {
+    if (K < 5) dst64[K * kBlk] = v;
+    else dst32[(K - 5) * kBlk] = (float)v;
+  }
+};
+
+__device__ __forceinline__ void cp_async16(void* smemDst, const void* gmemSrc)
+{
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smemDst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmemSrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// The warp copies `bytes` (a multiple of 16) from global to shared memory,
+// 16 bytes per lane per round.
+__device__ __forceinline__ void warp_copy(unsigned char* dst, const unsigned char* src, int bytes, int lane)
+{
+  for (int c = lane * 16; c < bytes; c += 32 * 16) cp_async16(dst + c, src + c);
+}
+
+// Copies tile t's state block (and, mixed, weight block) into buf.
+template <bool MIXED>
+__device__ __forceinline__ void stage_tile(const StepArgs& a, int t, int lane, unsigned char* buf)
+{
+  const WarpTile tile = a.tiles[t];
+  const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
+  const int64_t b = tile.first / kBlk;
+  if (MIXED) {
+    warp_copy(buf, (const unsigned char*)(Tp->s64 + b * kRowsMixed64 * kBlk), kRowsMixed64 * kBlk * 8, lane);
+    warp_copy(buf + kRowsMixed64 * kBlk * 8, (const unsigned char*)(Tp->s32 + b * kRowsMixed32 * kBlk),
+              kRowsMixed32 * kBlk * 4, lane);
+    if (Tp->scale != 0.0) {
+      const int wr = weight_rows(Tp->cls, true);
+      warp_copy(buf + kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4,
+                (const unsigned char*)((const float*)Tp->w + b * wr * kBlk), wr * kBlk * 4, lane);
+    }
+  } else {
+    warp_copy(buf, (const unsigned char*)(Tp->s64 + b * kRows64 * kBlk), kRows64 * kBlk * 8, lane);
+  }
+}
+
+// One tile.  With `staged` the tile's state (and mixed weights) are read
+// from buf; otherwise straight from global memory.
 template <bool MIXED, int SLOT>
-__global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(StepArgs a)
+__device__ __forceinline__ void step_tile(const StepArgs& a, int t, int lane, const unsigned char* buf, bool staged)
 {
   constexpr bool SPEC = SLOT >= 0;
-  const int warp = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
-  if (warp >= a.nTiles) return;   // whole warps leave together
-  const int lane = threadIdx.x & 31;
-  const WarpTile tile = a.tiles[warp];
+  const WarpTile tile = a.tiles[t];
   const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
   const int64_t lstep = Tp->step0 + a.k;
   const double time = a.times[lstep];
@@ -180,8 +254,8 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
   for (int k = 0; k < nstim; ++k) {
     const double v = __shfl_sync(0xffffffffu, stimVal, k);
     if (v != 0.0) {
-      const cdb_stimulus* b = a.stims + stim0 + k;
-      if (x > b->xMin && x < b->xMax && y > b->yMin && y < b->yMax && z > b->zMin && z < b->zMax) istim = v;
+      const cdb_stimulus* bx = a.stims + stim0 + k;
+      if (x > bx->xMin && x < bx->xMax && y > bx->yMin && y < bx->yMax && z > bx->zMin && z < bx->zMax) istim = v;
     }
   }
   double vnew = 0.0;
@@ -189,40 +263,43 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
     const int cur = (Tp->parity + a.k) & 1;
     const double* __restrict__ vin = Tp->vm[cur];
     double* __restrict__ vout = Tp->vm[cur ^ 1];
-    const int64_t n = Tp->n;   // tissues hold fewer than 2^31 cells
     const double scale = Tp->scale;
     const int cls = Tp->cls;
-    const void* wp = Tp->w;
     const BlockScale blk = Tp->blk;
-    double* const s64 = Tp->s64 + i;
-    float* const s32 = Tp->s32 + i;
-    double* const act = Tp->act;
+    const int64_t b = i / kBlk;
+    const int pos = (int)(i - b * kBlk);
     const double phi0 = vin[vox];
 
     double dvmD = 0.0;
     if (scale != 0.0) {
       double acc;
       if (MIXED) {
-        const float* w = (const float*)wp;
-        acc = cls == kVolume ? stencil32<kVolume>(w, n, g.px, g.pxy, vin, vox, phi0, i)
-            : cls == kSheet ? stencil32<kSheet>(w, n, g.px, g.pxy, vin, vox, phi0, i)
-                            : stencil32<kCable>(w, n, g.px, g.pxy, vin, vox, phi0, i);
+        const int wr = weight_rows(cls, true);
+        const float* w = staged ? (const float*)(buf + kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4) + pos
+                                : (const float*)Tp->w + b * wr * kBlk + pos;
+        acc = cls == kVolume ? stencil32<kVolume>(w, g.px, g.pxy, vin, vox, phi0)
+            : cls == kSheet ? stencil32<kSheet>(w, g.px, g.pxy, vin, vox, phi0)
+                            : stencil32<kCable>(w, g.px, g.pxy, vin, vox, phi0);
       } else {
-        const double* w = (const double*)wp;
-        acc = cls == kVolume ? stencil64<kVolume>(w, n, g.px, g.pxy, vin, vox, phi0, i)
-            : cls == kSheet ? stencil64<kSheet>(w, n, g.px, g.pxy, vin, vox, phi0, i)
-                            : stencil64<kCable>(w, n, g.px, g.pxy, vin, vox, phi0, i);
+        const int wr = weight_rows(cls, false);
+        const double* w = (const double*)Tp->w + b * wr * kBlk + pos;
+        acc = cls == kVolume ? stencil64<kVolume>(w, g.px, g.pxy, vin, vox, phi0)
+            : cls == kSheet ? stencil64<kSheet>(w, g.px, g.pxy, vin, vox, phi0)
+                            : stencil64<kCable>(w, g.px, g.pxy, vin, vox, phi0);
       }
       dvmD = acc * scale;
     }
 
-    // With SPEC the slot is a template parameter, so every coefficient is
-    // an immediate constant-bank operand of its FMA (no load instruction).
+    // With SPEC the slot is a template parameter, so every coefficient
+    // address is a compile-time constant.
     const int rt = SPEC ? SLOT : a.rt;
     const double* c64 = c_coef64 + rt * kFitPoolPerType;
     double dvmR;
     if (MIXED) {
-      IOMixed io{s64, s32, n};
+      double* g64 = Tp->s64 + b * kRowsMixed64 * kBlk + pos;
+      float* g32 = Tp->s32 + b * kRowsMixed32 * kBlk + pos;
+      IOBlockMixed io{staged ? (const double*)buf + pos : g64,
+                      staged ? (const float*)(buf + kRowsMixed64 * kBlk * 8) + pos : g32, g64, g32};
       const float* c32 = c_coef32 + rt * kFitPoolPerType;
       if (SPEC) {
         SpecFits fits{c64, c32};
@@ -232,7 +309,8 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
         dvmR = (double)tt06_step_mixed(c_scal[rt], blk, fits, (float)a.dt, phi0, io);
       }
     } else {
-      IO64 io{s64, n};
+      double* g64 = Tp->s64 + b * kRows64 * kBlk + pos;
+      IOBlock64 io{staged ? (const double*)buf + pos : g64, g64};
       if (SPEC) {
         SpecFits fits{c64, nullptr};
         dvmR = tt06_step(c_scal[rt], blk, fits, a.dt, phi0, io);
@@ -245,7 +323,7 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
     vnew = phi0 + a.dt * (dvmR + dvmD + istim);
     vout[vox] = vnew;
     if (vnew > 0.0) {
-      double* ap = act + i;
+      double* ap = Tp->act + i;
       if (*ap < 0.0) *ap = tnext;
     }
   }
@@ -261,6 +339,51 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
       atomicMax(Tp->minmax + 1, ordered_bits(hi));
     }
   }
+}
+
+// Resident CTAs per SM the register budget aims at: 4 CTAs (16 warps, 128
+// registers).  The mixed step fits without spilling; the FP64 step spills
+// ~90 bytes per thread to L1 there, and still runs 1.2x faster on B200 than
+// at 3 CTAs (168 registers, no spill) because latency hiding dominates.
+#ifndef CDB_FP64_MIN_CTAS
+#define CDB_FP64_MIN_CTAS 4
+#endif
+template <bool MIXED>
+constexpr int min_ctas() { return MIXED ? 4 : CDB_FP64_MIN_CTAS; }
+
+// Persistent over the launch's warp tiles: warp w takes tiles w, w + W,
+// w + 2W, ... (W warps in the grid).  With a.stage set, the next tile's
+// state (and mixed weights) is in flight to shared memory while the current
+// one computes.
+// SLOT >= 0: the launch's reaction type is constant-memory slot SLOT and its
+// fits have the compiled shapes (fit_shapes.h); SLOT < 0: any slot (a.rt)
+// with run-time shapes.
+template <bool MIXED, int SLOT>
+__global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(StepArgs a)
+{
+  constexpr int kBuf = stage_bytes<MIXED>();
+  __shared__ __align__(16) unsigned char smem[kWarpsPerCta * 2 * kBuf];
+  const int lane = threadIdx.x & 31;
+  const int warpInCta = threadIdx.x >> 5;
+  unsigned char* mine = smem + warpInCta * 2 * kBuf;
+  const int stride = gridDim.x * kWarpsPerCta;
+  int t = blockIdx.x * kWarpsPerCta + warpInCta;
+  if (!a.stage) {
+    for (; t < a.nTiles; t += stride) step_tile<MIXED, SLOT>(a, t, lane, nullptr, false);
+    return;
+  }
+  if (t < a.nTiles) stage_tile<MIXED>(a, t, lane, mine);
+  cp_async_commit();
+  for (int it = 0; t < a.nTiles; ++it, t += stride) {
+    const int tn = t + stride;
+    __syncwarp();   // every lane is done with the buffer refilled next
+    if (tn < a.nTiles) stage_tile<MIXED>(a, tn, lane, mine + ((it + 1) & 1) * kBuf);
+    cp_async_commit();
+    cp_async_wait_prev();   // this thread's copies of tile t have landed
+    __syncwarp();           // and so have the other lanes'
+    step_tile<MIXED, SLOT>(a, t, lane, mine + (it & 1) * kBuf, true);
+  }
+  cp_async_wait_all();
 }
 
 // One step of one reaction type: the compiled kernel of its slot when the
@@ -301,6 +424,12 @@ __global__ void reset_minmax_kernel(TissueDev* tissues, int nTissues)
 
 // ---- set-up kernels ----
 
+// AoSoA index of row r of cell i
+__host__ __device__ inline int64_t aosoa(int64_t i, int rows, int r)
+{
+  return ((i / kBlk) * rows + r) * kBlk + (i % kBlk);
+}
+
 // Marks tissue voxels of the full-padded build block with their cell index.
 __global__ void build_voxel_map_kernel(int64_t n, const int64_t* __restrict__ gid, int nx, int ny, int64_t bx,
                                        int64_t bxy, int64_t* __restrict__ map, int64_t* __restrict__ cellVoxel)
@@ -314,8 +443,8 @@ __global__ void build_voxel_map_kernel(int64_t n, const int64_t* __restrict__ gi
   cellVoxel[i] = v;
 }
 
-// Weights of every cell (fgr_cell_weights), written in the tissue's class
-// layout: FP64 rows = A0 then the class nodes; mixed rows = class nodes.
+// Weights of every cell (fgr_cell_weights), written AoSoA in the tissue's
+// class layout: FP64 rows = A0 then the class nodes; mixed rows = class nodes.
 __global__ void build_weights_kernel(int64_t n, const int64_t* __restrict__ map, const int64_t* __restrict__ cellVoxel,
                                      const double* __restrict__ sigma6, int64_t bx, int64_t bxy, double hx, double hy,
                                      double hz, int cls, int mixed, void* __restrict__ wout)
@@ -335,11 +464,11 @@ __global__ void build_weights_kernel(int64_t n, const int64_t* __restrict__ map,
   const int rows = class_rows(cls);
   if (mixed) {
     float* w = (float*)wout;
-    for (int r = 1; r < rows; ++r) w[(r - 1) * n + i] = (float)W[class_node(cls, r)];
+    for (int r = 1; r < rows; ++r) w[aosoa(i, rows - 1, r - 1)] = (float)W[class_node(cls, r)];
   } else {
     double* w = (double*)wout;
-    w[i] = W[0];
-    for (int r = 1; r < rows; ++r) w[r * n + i] = W[class_node(cls, r)];
+    w[aosoa(i, rows, 0)] = W[0];
+    for (int r = 1; r < rows; ++r) w[aosoa(i, rows, r)] = W[class_node(cls, r)];
   }
 }
 
@@ -368,17 +497,40 @@ __global__ void gather_vm_kernel(int64_t n, const double* __restrict__ blk, doub
   if (i < n) dst[i] = blk[cell_voxel(i, voxel, nx, ny, px, pxy, py0, pz0)];
 }
 
-__global__ void init_state_kernel(int64_t n, double* s64, float* s32, int mixed, double* act)
+// Row var of the AoSoA state to / from a cell-order array of doubles.
+__global__ void gather_state_kernel(int64_t n, const double* __restrict__ s64, const float* __restrict__ s32,
+                                    int mixed, int var, double* __restrict__ dst)
 {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (!mixed) dst[i] = s64[aosoa(i, kRows64, var)];
+  else if (var < kRowsMixed64) dst[i] = s64[aosoa(i, kRowsMixed64, var)];
+  else dst[i] = (double)s32[aosoa(i, kRowsMixed32, var - kRowsMixed64)];
+}
+
+__global__ void scatter_state_kernel(int64_t n, double* __restrict__ s64, float* __restrict__ s32, int mixed, int var,
+                                     const double* __restrict__ src)
+{
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (!mixed) s64[aosoa(i, kRows64, var)] = src[i];
+  else if (var < kRowsMixed64) s64[aosoa(i, kRowsMixed64, var)] = src[i];
+  else s32[aosoa(i, kRowsMixed32, var - kRowsMixed64)] = (float)src[i];
+}
+
+// Initial state of every cell of the padded block count (pad cells too).
+__global__ void init_state_kernel(int64_t nPad, double* s64, float* s32, int mixed, double* act, int64_t n)
+{
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nPad) return;
   if (mixed) {
-    for (int k = 0; k < 5; ++k) s64[k * n + i] = tt06_initial_state(k);
-    for (int k = 5; k < kNumStates; ++k) s32[(k - 5) * n + i] = (float)tt06_initial_state(k);
+    for (int k = 0; k < kRowsMixed64; ++k) s64[aosoa(i, kRowsMixed64, k)] = tt06_initial_state(k);
+    for (int k = kRowsMixed64; k < kNumStates; ++k)
+      s32[aosoa(i, kRowsMixed32, k - kRowsMixed64)] = (float)tt06_initial_state(k);
   } else {
-    for (int k = 0; k < kNumStates; ++k) s64[k * n + i] = tt06_initial_state(k);
+    for (int k = 0; k < kNumStates; ++k) s64[aosoa(i, kRows64, k)] = tt06_initial_state(k);
   }
-  act[i] = -1.0;
+  if (i < n) act[i] = -1.0;
 }
 
 __global__ void fill_kernel(int64_t n, double* p, double v)

@@ -159,6 +159,41 @@ __device__ __forceinline__ float fit_spec32(const float* __restrict__ c, float x
   return __fdividef(num, den);
 }
 
+// FP32 fits of V in the power basis: with pw[k] = V^k computed once per
+// cell (shared by every V-fit), each term is fma(pw[k], c_k, acc), so the
+// coefficient is the multiplicand and can be an immediate constant-bank
+// operand; Horner's form puts it in the addend slot, where it needs a load.
+// Used only for the fits the FP32 error check accepted (well conditioned
+// in the monomial basis, so the two summation orders agree to FP32 rounding).
+constexpr int kMaxPow = 24;
+
+template <int SLOT>
+__device__ __forceinline__ float fit_pow32(const float* __restrict__ c, const float (&pw)[kMaxPow])
+{
+  constexpr int N = kSpecNumer[SLOT], D = kSpecDenom[SLOT], O = kSpecOffset[SLOT];
+  static_assert(N <= kMaxPow && D <= kMaxPow, "power table too short");
+  float num = c[O];
+#pragma unroll
+  for (int k = 1; k < N; ++k) num = fmaf(pw[k], c[O + k], num);
+  if (D == 1) return num;
+  float den = fmaf(pw[1], c[O + N], 1.0f);
+#pragma unroll
+  for (int k = 2; k < D; ++k) den = fmaf(pw[k], c[O + N + k - 1], den);
+  return __fdividef(num, den);
+}
+
+// The largest power any FP32-evaluated V-fit of the compiled shapes needs.
+__host__ __device__ constexpr int spec_max_pow32()
+{
+  int m = 1;
+  for (int s = 1; s < 30; ++s) {
+    if (s == 29 || ((kSpecFp64Mask >> s) & 1u)) continue;   // K1 takes V - E_K; FP64 fits use Horner
+    const int need = kSpecNumer[s] > kSpecDenom[s] ? kSpecNumer[s] : kSpecDenom[s];
+    if (need > m) m = need;
+  }
+  return m;
+}
+
 // Fit evaluation policies.  c64 / c32 point at one reaction type's
 // coefficient pool (FP64 and FP32 copies).
 struct GenericFits {
@@ -176,11 +211,21 @@ struct GenericFits {
     if ((sh->fp64mask >> SLOT) & 1u) return (float)f64<SLOT>(xd);
     return fit_eval_fast(c32 + sh->offset[SLOT], sh->numer[SLOT], sh->denom[SLOT], xf);
   }
+  __device__ __forceinline__ void set_v(float) {}
+  template <int SLOT>
+  __device__ __forceinline__ float fv(double vd) const { return fmix<SLOT>((float)vd, vd); }
 };
 
 struct SpecFits {
   const double* __restrict__ c64;
   const float* __restrict__ c32;
+  float pw[kMaxPow];   // V^k for the FP32 V-fits (set_v)
+  __device__ __forceinline__ void set_v(float v)
+  {
+    pw[0] = 1.0f;
+#pragma unroll
+    for (int k = 1; k < spec_max_pow32(); ++k) pw[k] = pw[k - 1] * v;
+  }
   template <int SLOT>
   __device__ __forceinline__ double f64(double x) const { return fit_spec64<SLOT>(c64, x); }
   template <int SLOT>
@@ -188,6 +233,13 @@ struct SpecFits {
   {
     if ((kSpecFp64Mask >> SLOT) & 1u) return (float)fit_spec64<SLOT>(c64, xd);
     return fit_spec32<SLOT>(c32, xf);
+  }
+  // a fit of V: the power basis in FP32
+  template <int SLOT>
+  __device__ __forceinline__ float fv(double vd) const
+  {
+    if ((kSpecFp64Mask >> SLOT) & 1u) return (float)fit_spec64<SLOT>(c64, vd);
+    return fit_pow32<SLOT>(c32, pw);
   }
 };
 

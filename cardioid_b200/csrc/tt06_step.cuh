@@ -119,12 +119,13 @@ __device__ __forceinline__ double tt06_step(const TT06Scalars& p, const BlockSca
 
 // Mixed step.  Returns dVm = -Iion in float.
 template <class Fits, class IO>
-__device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const BlockScale& blk, const Fits& fits,
+__device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const BlockScale& blk, Fits& fits,
                                                  float dtf, double V, IO& io)
 {
-  // every V-fit takes V; its FP32 argument is Vf
-#define FIT(slot, x) fits.template fmix<slot>(x, V)
+  // every V-fit takes V (fv: the power basis where the policy has one)
+#define FIT(slot, x) fits.template fv<slot>(V)
 #define FITX(slot, xf, xd) fits.template fmix<slot>(xf, xd)
+  fits.set_v((float)V);
   constexpr float Cm = 0.185f, F = 96485.3415f, RT = 8314.472f * 310.0f, Vc = 0.016404f, Cao = 2.0f;
   constexpr float BufC = 0.2f, BufSr = 10.0f, BufSs = 0.4f, EC2 = 1.5f * 1.5f;
   constexpr float KbufC = 0.001f, KbufSr = 0.3f, KbufSs = 0.00025f, Kup2 = 0.00025f * 0.00025f;
@@ -148,12 +149,14 @@ __device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const Blo
 
   // currents
   const float calT3 = FIT(F_CalT3, Vf), calT4 = FIT(F_CalT4, Vf);
-  const float eCa = 0.5f * RT_F * logf(__fdividef(Cao, caI));
+  // __logf (hardware log2, ~2^-21 relative): the Nernst potentials need
+  // ~1e-6 mV, and their arguments are positive concentration ratios
+  const float eCa = 0.5f * RT_F * __logf(__fdividef(Cao, caI));
   const float iBCa = (float)p.g_bca * (Vf - eCa);
   const float iPCa = __fdividef(caI * (float)p.g_pCa, caI + KpCa);
   const float expG = FIT(F_expG, Vf), expGm1 = FIT(F_expGm1, Vf);
   const float pKterm = FIT(F_pKterm, Vf);
-  const float eK = RT_F * logf(__fdividef(Ko, kI));
+  const float eK = RT_F * __logf(__fdividef(Ko, kI));
   const float naKterm = FIT(F_NaKterm, Vf);
   const float iNaK = __fdividef(naI * naKterm, naI + KmNa);
   const float vEK = Vf - eK;
@@ -179,8 +182,8 @@ __device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const Blo
   const float iK1 = FITX(F_K1, vEK, V - (double)eK);
   const float iPK = vEK * (float)p.g_pK * pKterm;
   const float iKr = 0.430331482911935f * 2.3237900077f * vEK * Xr1 * Xr2 * gKr;
-  const float eNa = RT_F * logf(__fdividef(Nao, naI));
-  const float eKs = RT_F * logf(__fdividef(Ko + Nao * Pkna, kI + naI * Pkna));
+  const float eNa = RT_F * __logf(__fdividef(Nao, naI));
+  const float eKs = RT_F * __logf(__fdividef(Ko + Nao * Pkna, kI + naI * Pkna));
   const float iKs = (Xs * Xs) * (float)p.g_Ks * (Vf - eKs);
   const float iBNa = (float)p.g_bna * (Vf - eNa);
   const float iTo = vEK * (float)p.g_to * r * s;

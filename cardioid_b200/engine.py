@@ -191,6 +191,16 @@ class Engine:
     def step_host(self, tid, vm_in, vm_out):
         _lib.check(_lib.load().cdb_engine_step_host(self.h, tid, _lib.dptr(vm_in), _lib.dptr(vm_out)))
 
+    def set_tuning(self, stage, ctas_per_sm):
+        """stage: 1 = copy each warp's next tile into shared memory while it
+        computes the current one; ctas_per_sm sizes the persistent grid."""
+        _lib.check(_lib.load().cdb_engine_set_tuning(self.h, int(stage), int(ctas_per_sm)))
+
+    def get_tuning(self):
+        p, c = ctypes.c_int32(), ctypes.c_int32()
+        _lib.check(_lib.load().cdb_engine_get_tuning(self.h, ctypes.byref(p), ctypes.byref(c)))
+        return p.value, c.value
+
     def launch_count(self):
         c = ctypes.c_int64()
         _lib.check(_lib.load().cdb_engine_launch_count(self.h, ctypes.byref(c)))

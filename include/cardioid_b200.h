@@ -217,6 +217,15 @@ cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, 
  * measuring it against IEEE division.  No counterpart in the reference. */
 cdb_status cdb_diag_div64(int device, int64_t n, const double* a, const double* b, double* q, void* stream);
 
+/* Launch tuning of the step kernel (no counterpart in the reference):
+ * stage 1 = each warp copies its next tile's state (mixed: and weights)
+ * into shared memory with cp.async while it computes the current one, 0 =
+ * direct loads; ctasPerSm sizes the persistent grid (SMs x ctasPerSm CTAs
+ * of 128 threads).  Defaults 1 and 4; cardioid_b200.autotune picks them by
+ * timing. */
+cdb_status cdb_engine_set_tuning(cdb_engine* e, int32_t stage, int32_t ctasPerSm);
+cdb_status cdb_engine_get_tuning(cdb_engine* e, int32_t* stage, int32_t* ctasPerSm);
+
 /* Kernels launched by this engine since creation. */
 cdb_status cdb_engine_launch_count(cdb_engine* e, int64_t* launches);
 /* The CUDA stream (cudaStream_t) the engine launches on. */
