@@ -240,7 +240,8 @@ def run_ours(args):
     n = t.n
     peak, peak_src = read_peaks()
     results = {}
-    for prec in ("fp64", "mixed"):
+    precs = ("fp64", "mixed") if args.precision == "both" else (args.precision,)
+    for prec in precs:
         with engine.Engine(DT, precision=prec, device=local) as e:
             rx, _ = engine.transmural_setup(e, t, DT)
             e.add_tissue(t, rx)
@@ -257,7 +258,7 @@ def run_ours(args):
                              "algorithmic_bytes_per_cell_step": ALGO_BYTES[prec],
                              "traffic": (traffic_pc * n if traffic_pc else None)},
             }
-            if prec == "mixed":
+            if prec == "mixed" and not args.no_e2e:
                 # end to end through the C ABI with host buffers: every step
                 # copies Vm in from pinned host memory and the new Vm back
                 vin = torch.from_numpy(t.vm0.copy()).pin_memory()
@@ -277,6 +278,12 @@ def run_ours(args):
                                   "steps": e2e_steps,
                                   "call": "cdb_engine_step_host (pinned host Vm in, one fused step, host Vm out)"}
     if rank != 0:
+        return
+    if args.precision != "both" or args.no_e2e:
+        # a profiling run: one line per precision, no headline
+        for prec in precs:
+            print(json.dumps({"config": w["label"], "precision": prec, "steps": args.steps, **results[prec]}),
+                  flush=True)
         return
     m, f = results["mixed"], results["fp64"]
     line = {
@@ -323,13 +330,16 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=["box256", "box128", "box64"], default="box256")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", choices=["both", "fp64", "mixed"], default="both",
+                    help="profiling runs: time one precision only (no headline line)")
+    ap.add_argument("--no-e2e", action="store_true", help="profiling runs: skip the end-to-end loop")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

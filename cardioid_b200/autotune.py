@@ -9,7 +9,7 @@ of the same shape.
 import itertools
 
 STAGE_MODES = (0, 1)
-CTAS_PER_SM = (4, 8)
+CTAS_PER_SM = (0, 4, 8)     # 0: as many as are resident
 
 
 def time_steps(eng, steps):

@@ -67,7 +67,7 @@ struct HostTissue {
   TissueDev dev{};
   std::vector<cdb_stimulus> stims;
   DeviceBuffer vm0, vm1, s64, s32, w, voxel, act, minmax;
-  std::vector<uint8_t> slotOf;   // constant-memory slot of each cell
+  std::vector<WarpTile> tiles[CDB_MAX_REACTION_TYPES];   // by slot; .tissue set at rebuild
   int64_t steps = 0;       // steps taken
   int parity = 0;
   int64_t n = 0;
@@ -122,8 +122,17 @@ struct Engine {
   bool graphMinmax = false;
   // launch tuning (cdb_engine_set_tuning; the autotuner picks them)
   int stage = 1;           // 1: stage each warp's next tile through shared memory (cp.async)
-  int ctasPerSm = 4;       // persistent grid: SMs x this
+  int ctasPerSm = 0;       // persistent grid: SMs x this; 0 = as many as are resident
   int numSms = 148;
+  int resident[CDB_MAX_REACTION_TYPES + 1] = {};   // resident CTAs per SM by slot (last: generic)
+
+  int grid_ctas_per_sm(int slot)
+  {
+    if (ctasPerSm > 0) return ctasPerSm;
+    int& r = resident[slot < 0 ? CDB_MAX_REACTION_TYPES : slot];
+    if (r == 0) r = cfg.precision == CDB_MIXED ? resident_ctas<true>(slot) : resident_ctas<false>(slot);
+    return r > 0 ? r : 4;
+  }
 
   ~Engine()
   {
@@ -168,21 +177,11 @@ struct Engine {
       const int idx = (int)devs.size();
       devs.push_back(t.dev);
       order.push_back(kv.first);
-      // runs of one reaction type, cut into warp tiles of at most 32 cells
-      int64_t f = 0;
-      while (f < t.n) {
-        const uint8_t slot = t.slotOf[f];
-        int64_t e = f + 1;
-        // a tile never crosses a 32-cell AoSoA block
-        const int64_t blockEnd = (f / kBlk + 1) * kBlk;
-        while (e < t.n && e < blockEnd && t.slotOf[e] == slot) ++e;
-        WarpTile tl;
-        tl.tissue = idx;
-        tl.first = f;
-        tl.count = (int)(e - f);
-        bySlot[slot].push_back(tl);
-        f = e;
-      }
+      for (int sl = 0; sl < CDB_MAX_REACTION_TYPES; ++sl)
+        for (WarpTile tl : t.tiles[sl]) {
+          tl.tissue = idx;
+          bySlot[sl].push_back(tl);
+        }
     }
     slotTiles.clear();
     for (int sl = 0; sl < CDB_MAX_REACTION_TYPES; ++sl) {
@@ -205,13 +204,24 @@ struct Engine {
     return CDB_OK;
   }
 
-  // Host copies of step0/parity follow the device ones (advance_kernel).
+  // Host copies of step0/parity/actAll follow the device ones (advance_kernel).
   void advance_host(int k)
   {
     for (auto& kv : tissues) {
       kv.second->steps += k;
       kv.second->parity = (kv.second->parity + k) & 1;
+      kv.second->dev.actAll = 0;
     }
+  }
+
+  // Device address of a tissue's actAll flag; null while the tables are
+  // stale (the next rebuild uploads the host copy).
+  int* act_all_flag(int id)
+  {
+    if (dirty) return nullptr;
+    for (size_t k = 0; k < order.size(); ++k)
+      if (order[k] == id) return &dTissues.as<TissueDev>()[k].actAll;
+    return nullptr;
   }
 
   cdb_status launch_batch(int k, bool minmax)
@@ -234,9 +244,9 @@ struct Engine {
         a.k = s;
         a.minmax = (minmax && s == k - 1) ? 1 : 0;
         a.stage = stage;
-        const unsigned grid = (unsigned)std::min<int64_t>(grid_for(a.nTiles, kWarpsPerCta),
-                                                          (int64_t)numSms * ctasPerSm);
         const int slot = spec[st.first] ? st.first : -1;
+        const unsigned grid = (unsigned)std::min<int64_t>(grid_for(a.nTiles, kWarpsPerCta),
+                                                          (int64_t)numSms * grid_ctas_per_sm(slot));
         if (cfg.precision == CDB_MIXED) launch_step<true>(slot, grid, stream, a);
         else launch_step<false>(slot, grid, stream, a);
         ++launches;
@@ -395,6 +405,8 @@ cdb_status cdb_engine_create(const cdb_engine_config* cfg, cdb_engine** out)
   e->e.cfg = *cfg;
   CDB_CUDA(cudaStreamCreateWithFlags(&e->e.stream, cudaStreamNonBlocking));
   CDB_CUDA(cudaDeviceGetAttribute(&e->e.numSms, cudaDevAttrMultiProcessorCount, cfg->device));
+  // measured on the 256^3 box: staging pays for the mixed step, not for FP64
+  e->e.stage = cfg->precision == CDB_MIXED ? 1 : 0;
   *out = e.release();
   return CDB_OK;
 }
@@ -403,7 +415,7 @@ cdb_status cdb_engine_set_tuning(cdb_engine* e, int32_t stage, int32_t ctasPerSm
 {
   CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
   CDB_CHECK(stage == 0 || stage == 1, CDB_INVALID_ARG, "stage must be 0 or 1");
-  CDB_CHECK(ctasPerSm >= 1 && ctasPerSm <= 64, CDB_INVALID_ARG, "ctasPerSm must be in [1, 64]");
+  CDB_CHECK(ctasPerSm >= 0 && ctasPerSm <= 64, CDB_INVALID_ARG, "ctasPerSm must be in [0, 64]");
   Engine& E = e->e;
   CDB_CUDA(cudaSetDevice(E.cfg.device));
   CDB_CUDA(cudaStreamSynchronize(E.stream));
@@ -484,6 +496,37 @@ cdb_status cdb_engine_free_bytes(cdb_engine* e, int64_t* freeBytes, int64_t* tot
   return CDB_OK;
 }
 
+// A tissue's warp tiles, by constant-memory slot: runs of cells that share
+// a reaction type, lie in one 32-cell AoSoA block and occupy consecutive
+// voxels of one grid row (gid = x + nx (y + ny z); NULL gid = all cells).
+void build_tiles(HostTissue& h, const int64_t* gid, const uint8_t* reaction, const int* slots)
+{
+  const TissueDev& d = h.dev;
+  for (auto& v : h.tiles) v.clear();
+  int64_t f = 0;
+  while (f < h.n) {
+    const int slot = slots[reaction[f]];
+    const int64_t g0 = gid ? gid[f] : f;
+    const int x0 = (int)(g0 % h.nx);
+    const int64_t yz = g0 / h.nx;
+    const int y = (int)(yz % h.ny), z = (int)(yz / h.ny);
+    const int64_t blockEnd = (f / kBlk + 1) * kBlk;
+    int64_t e = f + 1;
+    while (e < h.n && e < blockEnd && slots[reaction[e]] == slot && x0 + (e - f) < h.nx &&
+           (gid ? gid[e] : e) == g0 + (e - f))
+      ++e;
+    WarpTile tl{};
+    tl.first = f;
+    tl.count = (int)(e - f);
+    tl.vox0 = (int64_t)(x0 + 1) + d.px * (int64_t)(y + d.py0) + d.pxy * (int64_t)(z + d.pz0);
+    tl.x0 = x0;
+    tl.y = y;
+    tl.z = z;
+    h.tiles[slot].push_back(tl);
+    f = e;
+  }
+}
+
 cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_t* id)
 {
   CDB_CHECK(e && id, CDB_INVALID_ARG, "null argument");
@@ -561,9 +604,7 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
       CDB_CUDA(cudaMemcpyAsync(h->voxel.p, v.data(), n * 8, cudaMemcpyHostToDevice, s));
       CDB_CUDA(cudaStreamSynchronize(s));
     }
-    // per-cell reaction ids -> this engine's constant-memory slots
-    h->slotOf.resize(n);
-    for (int64_t i = 0; i < n; ++i) h->slotOf[i] = (uint8_t)E.slots[t->reaction[i]];
+    build_tiles(*h, t->gid, t->reaction, E.slots);
     CDB_CUDA(cudaStreamSynchronize(s));
   }
   d.vm[0] = h->vm0.as<double>();
@@ -574,6 +615,7 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
   d.voxel = masked ? h->voxel.as<int64_t>() : nullptr;
   d.act = h->act.as<double>();
   d.minmax = h->minmax.as<unsigned long long>();
+  d.actAll = 1;
   init_state_kernel<<<grid_for(nPad, 256), 256, 0, s>>>(nPad, d.s64, d.s32, mixed ? 1 : 0, d.act, n);
   E.launches += 1;
   {
@@ -586,7 +628,7 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
       E.launches += 1;
     }
     scatter_vm_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, v0.as<double>(), d.vm[0], d.voxel, d.nx, d.ny, d.px,
-                                                       d.pxy, d.py0, d.pz0);
+                                                       d.pxy, d.py0, d.pz0, nullptr);
     E.launches += 1;
     CDB_CUDA(cudaStreamSynchronize(s));
   }
@@ -668,8 +710,10 @@ cdb_status cdb_engine_write_vm(cdb_engine* e, int32_t id, const double* host)
   CDB_CUDA(tmp.alloc(t->n * 8));
   CDB_CUDA(cudaMemcpyAsync(tmp.p, host, t->n * 8, cudaMemcpyHostToDevice, E.stream));
   const TissueDev& d = t->dev;
+  t->dev.actAll = 1;
   scatter_vm_kernel<<<grid_for(t->n, 256), 256, 0, E.stream>>>(t->n, tmp.as<double>(), d.vm[t->parity], d.voxel,
-                                                              d.nx, d.ny, d.px, d.pxy, d.py0, d.pz0);
+                                                              d.nx, d.ny, d.px, d.pxy, d.py0, d.pz0,
+                                                              E.act_all_flag(id));
   E.launches += 1;
   CDB_CUDA(cudaStreamSynchronize(E.stream));
   return CDB_OK;
@@ -791,8 +835,9 @@ cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, 
   const TissueDev& d = t->dev;
   cudaStream_t s = E.stream;
   CDB_CUDA(cudaMemcpyAsync(E.dStage.p, vm_in, n * 8, cudaMemcpyHostToDevice, s));
+  t->dev.actAll = 1;
   scatter_vm_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, E.dStage.as<double>(), d.vm[t->parity], d.voxel, d.nx, d.ny,
-                                                     d.px, d.pxy, d.py0, d.pz0);
+                                                     d.px, d.pxy, d.py0, d.pz0, E.act_all_flag(id));
   E.launches += 1;
   cdb_status st = E.step(1, false);
   if (st != CDB_OK) return st;

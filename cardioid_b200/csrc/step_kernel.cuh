@@ -47,16 +47,23 @@ struct TissueDev {
   int cls;
   int nstim, stim0;
   int parity;             // buffer holding Vm at the start of the next launch batch
+  int actAll;             // Vm was written by the host since the last step
   int64_t step0;          // steps taken at the start of the next launch batch
   double scale;           // diffusionScale (0: no diffusion)
   BlockScale blk;
   unsigned long long* minmax;   // 2 slots
 };
 
+// A warp tile: up to 32 cells of one tissue that share a reaction type, lie
+// in one 32-cell AoSoA block and occupy consecutive voxels of one grid row,
+// so lane l's cell is first + l, its voxel vox0 + l, its x x0 + l.
 struct WarpTile {
   int tissue;
   int count;
   int64_t first;
+  int64_t vox0;           // padded-block voxel of the first cell
+  int x0, y, z;           // grid coordinates of the first cell
+  int pad;
 };
 
 struct StepArgs {
@@ -96,34 +103,6 @@ __device__ __forceinline__ double pulse_value(const cdb_stimulus& s, double time
   if (!(time > s.t0 && time < s.tf)) return 0.0;
   const double t = time - floor(time / s.period) * s.period;
   return (t >= s.phase && t < s.phase + s.duration) ? s.amplitude : 0.0;
-}
-
-// Geometry of one tissue, held in registers by the step kernel.
-struct Geom {
-  const int64_t* voxel;
-  int64_t px, pxy;
-  int nx, ny, py0, pz0;
-};
-
-__device__ __forceinline__ void cell_coords(const Geom& g, int64_t i, int64_t& vox, int& x, int& y, int& z)
-{
-  if (g.voxel) {
-    vox = g.voxel[i];
-    const int64_t yz = vox / g.px;
-    x = (int)(vox - yz * g.px) - 1;
-    const int64_t py = g.pxy / g.px;
-    const int64_t zz = yz / py;
-    y = (int)(yz - zz * py) - g.py0;
-    z = (int)zz - g.pz0;
-  } else {
-    const int nxy = g.nx * g.ny;
-    const int ii = (int)i;
-    z = ii / nxy;
-    const int r = ii - z * nxy;
-    y = r / g.nx;
-    x = r - y * g.nx;
-    vox = (int64_t)(x + 1) + g.px * (int64_t)(y + g.py0) + g.pxy * (int64_t)(z + g.pz0);
-  }
 }
 
 __device__ __forceinline__ int64_t node_offset(int64_t px, int64_t pxy, int node)
@@ -242,13 +221,11 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, int t, int lane, co
   const double stimVal = lane < nstim ? pulse_value(a.stims[stim0 + lane], time) : 0.0;
   const bool active = lane < tile.count;
   // lanes past the tile's end stand in for its first cell until the end
-  const int64_t i = tile.first + (active ? lane : 0);
-  Geom g;
-  g.voxel = Tp->voxel; g.px = Tp->px; g.pxy = Tp->pxy; g.nx = Tp->nx; g.ny = Tp->ny;
-  g.py0 = Tp->py0; g.pz0 = Tp->pz0;
-  int64_t vox;
-  int x, y, z;
-  cell_coords(g, i, vox, x, y, z);
+  const int l = active ? lane : 0;
+  const int64_t i = tile.first + l;
+  const int64_t vox = tile.vox0 + l;
+  const int x = tile.x0 + l, y = tile.y, z = tile.z;
+  const int64_t px = Tp->px, pxy = Tp->pxy;
   // iStim = 0, then every stimulus that is on assigns its value inside its box
   double istim = 0.0;
   for (int k = 0; k < nstim; ++k) {
@@ -277,15 +254,15 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, int t, int lane, co
         const int wr = weight_rows(cls, true);
         const float* w = staged ? (const float*)(buf + kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4) + pos
                                 : (const float*)Tp->w + b * wr * kBlk + pos;
-        acc = cls == kVolume ? stencil32<kVolume>(w, g.px, g.pxy, vin, vox, phi0)
-            : cls == kSheet ? stencil32<kSheet>(w, g.px, g.pxy, vin, vox, phi0)
-                            : stencil32<kCable>(w, g.px, g.pxy, vin, vox, phi0);
+        acc = cls == kVolume ? stencil32<kVolume>(w, px, pxy, vin, vox, phi0)
+            : cls == kSheet ? stencil32<kSheet>(w, px, pxy, vin, vox, phi0)
+                            : stencil32<kCable>(w, px, pxy, vin, vox, phi0);
       } else {
         const int wr = weight_rows(cls, false);
         const double* w = (const double*)Tp->w + b * wr * kBlk + pos;
-        acc = cls == kVolume ? stencil64<kVolume>(w, g.px, g.pxy, vin, vox, phi0)
-            : cls == kSheet ? stencil64<kSheet>(w, g.px, g.pxy, vin, vox, phi0)
-                            : stencil64<kCable>(w, g.px, g.pxy, vin, vox, phi0);
+        acc = cls == kVolume ? stencil64<kVolume>(w, px, pxy, vin, vox, phi0)
+            : cls == kSheet ? stencil64<kSheet>(w, px, pxy, vin, vox, phi0)
+                            : stencil64<kCable>(w, px, pxy, vin, vox, phi0);
       }
       dvmD = acc * scale;
     }
@@ -322,7 +299,11 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, int t, int lane, co
 
     vnew = phi0 + a.dt * (dvmR + dvmD + istim);
     vout[vox] = vnew;
-    if (vnew > 0.0) {
+    // Once Vm has gone above 0 the cell's activation time is set, so a cell
+    // with Vm > 0 at the start of the step already has one; only upward
+    // crossings need to read it, except in the first step after the host
+    // wrote Vm.
+    if (vnew > 0.0 && (phi0 <= 0.0 || (a.k == 0 && Tp->actAll))) {
       double* ap = Tp->act + i;
       if (*ap < 0.0) *ap = tnext;
     }
@@ -341,10 +322,9 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, int t, int lane, co
   }
 }
 
-// Resident CTAs per SM the register budget aims at: 4 CTAs (16 warps, 128
-// registers).  The mixed step fits without spilling; the FP64 step spills
-// ~90 bytes per thread to L1 there, and still runs 1.2x faster on B200 than
-// at 3 CTAs (168 registers, no spill) because latency hiding dominates.
+// Resident CTAs per SM the register budget aims at: at least 4 CTAs (16
+// warps, at most 128 registers).  Both steps fit there without spilling; the
+// mixed one uses few enough registers for 5 (shared memory then caps it).
 #ifndef CDB_FP64_MIN_CTAS
 #define CDB_FP64_MIN_CTAS 4
 #endif
@@ -386,21 +366,38 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
   cp_async_wait_all();
 }
 
-// One step of one reaction type: the compiled kernel of its slot when the
-// type has the compiled fit shapes (slot >= 0), else the generic kernel.
+// The compiled kernel of a slot when the type has the compiled fit shapes
+// (slot >= 0), else the generic kernel.
 template <bool MIXED>
-inline void launch_step(int slot, unsigned grid, cudaStream_t stream, const StepArgs& a)
+inline void (*step_kernel_for(int slot))(StepArgs)
 {
   static_assert(CDB_MAX_REACTION_TYPES == 6, "one compiled kernel per slot");
   switch (slot) {
-    case 0: fused_step_kernel<MIXED, 0><<<grid, kCta, 0, stream>>>(a); break;
-    case 1: fused_step_kernel<MIXED, 1><<<grid, kCta, 0, stream>>>(a); break;
-    case 2: fused_step_kernel<MIXED, 2><<<grid, kCta, 0, stream>>>(a); break;
-    case 3: fused_step_kernel<MIXED, 3><<<grid, kCta, 0, stream>>>(a); break;
-    case 4: fused_step_kernel<MIXED, 4><<<grid, kCta, 0, stream>>>(a); break;
-    case 5: fused_step_kernel<MIXED, 5><<<grid, kCta, 0, stream>>>(a); break;
-    default: fused_step_kernel<MIXED, -1><<<grid, kCta, 0, stream>>>(a); break;
+    case 0: return fused_step_kernel<MIXED, 0>;
+    case 1: return fused_step_kernel<MIXED, 1>;
+    case 2: return fused_step_kernel<MIXED, 2>;
+    case 3: return fused_step_kernel<MIXED, 3>;
+    case 4: return fused_step_kernel<MIXED, 4>;
+    case 5: return fused_step_kernel<MIXED, 5>;
+    default: return fused_step_kernel<MIXED, -1>;
   }
+}
+
+// One step of one reaction type.
+template <bool MIXED>
+inline void launch_step(int slot, unsigned grid, cudaStream_t stream, const StepArgs& a)
+{
+  step_kernel_for<MIXED>(slot)<<<grid, kCta, 0, stream>>>(a);
+}
+
+// CTAs of a slot's kernel that are resident on one SM at once (0 on error).
+template <bool MIXED>
+inline int resident_ctas(int slot)
+{
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel_for<MIXED>(slot), kCta, 0) != cudaSuccess)
+    return 0;
+  return n;
 }
 
 // After a launch batch of k steps: every tissue is k steps further.
@@ -410,6 +407,7 @@ __global__ void advance_kernel(TissueDev* tissues, int nTissues, int k)
   if (t < nTissues) {
     tissues[t].step0 += k;
     tissues[t].parity = (tissues[t].parity + k) & 1;
+    tissues[t].actAll = 0;
   }
 }
 
@@ -481,12 +479,15 @@ __device__ __forceinline__ int64_t cell_voxel(int64_t i, const int64_t* __restri
   return (x + 1) + px * (y + py0) + pxy * (z + pz0);
 }
 
+// Writes host-given Vm into a padded block; sets *actAll (when given) so the
+// next step checks every cell's activation time.
 __global__ void scatter_vm_kernel(int64_t n, const double* __restrict__ src, double* __restrict__ blk,
                                   const int64_t* __restrict__ voxel, int nx, int ny, int64_t px, int64_t pxy, int py0,
-                                  int pz0)
+                                  int pz0, int* actAll)
 {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i < n) blk[cell_voxel(i, voxel, nx, ny, px, pxy, py0, pz0)] = src[i];
+  if (i == 0 && actAll) *actAll = 1;
 }
 
 __global__ void gather_vm_kernel(int64_t n, const double* __restrict__ blk, double* __restrict__ dst,

@@ -193,7 +193,8 @@ class Engine:
 
     def set_tuning(self, stage, ctas_per_sm):
         """stage: 1 = copy each warp's next tile into shared memory while it
-        computes the current one; ctas_per_sm sizes the persistent grid."""
+        computes the current one; ctas_per_sm sizes the persistent grid
+        (0: as many CTAs per SM as are resident)."""
         _lib.check(_lib.load().cdb_engine_set_tuning(self.h, int(stage), int(ctas_per_sm)))
 
     def get_tuning(self):

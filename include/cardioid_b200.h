@@ -221,8 +221,9 @@ cdb_status cdb_diag_div64(int device, int64_t n, const double* a, const double* 
  * stage 1 = each warp copies its next tile's state (mixed: and weights)
  * into shared memory with cp.async while it computes the current one, 0 =
  * direct loads; ctasPerSm sizes the persistent grid (SMs x ctasPerSm CTAs
- * of 128 threads).  Defaults 1 and 4; cardioid_b200.autotune picks them by
- * timing. */
+ * of 128 threads), 0 = as many CTAs as are resident on an SM at once.
+ * Defaults: stage 1 for CDB_MIXED, 0 for CDB_FP64, ctasPerSm 0;
+ * cardioid_b200.autotune picks them by timing. */
 cdb_status cdb_engine_set_tuning(cdb_engine* e, int32_t stage, int32_t ctasPerSm);
 cdb_status cdb_engine_get_tuning(cdb_engine* e, int32_t* stage, int32_t* ctasPerSm);
 

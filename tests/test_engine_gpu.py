@@ -165,6 +165,46 @@ def test_step_host_equals_device_step(cdb_lib, fits002):
         np.testing.assert_array_equal(vm, ref)
 
 
+@pytest.mark.parametrize("graphs", [True, False])
+def test_activation_after_host_vm_writes(cdb_lib, oracle_port, fits002, graphs):
+    """The engine reads a cell's activation time only on upward crossings of
+    0 mV, plus every cell in the first step after the host wrote Vm.  Cells
+    the host puts above 0 mV (from the start, between steps, or through
+    cdb_engine_step_host) must still get the reference's activation time: the
+    first post-step time with Vm > 0."""
+    t = tissue.box(16, 12, 10)
+    x, _, _ = t.tuples()
+    far = np.flatnonzero(x >= 12)
+    t.vm0 = t.vm0.copy()
+    t.vm0[far[::41]] = 15.0
+    rx = _reaction_ids(t)
+    sim = oracle_port.PortSim(t, fits002, rx, DT)
+    with _engine(fits002, graphs=graphs) as e:
+        tid = e.add_tissue(t, rx)
+        e.step(30)
+        sim.step(30)
+        v = e.read_vm(tid)
+        v[far[7::29]] = 20.0
+        e.write_vm(tid, v)
+        sim.set_vm(v)
+        e.step(40)
+        sim.step(40)
+        v = e.read_vm(tid)
+        v[far[3::31]] = 25.0
+        out = np.empty_like(v)
+        e.step_host(tid, v, out)
+        sim.set_vm(v)
+        sim.step(1)
+        e.step(20)
+        sim.step(20)
+        act = e.read_activation(tid)
+        vm = e.read_vm(tid)
+    ref = sim.activation()
+    assert (ref[far[::41]] > 0).all() and (ref[far[7::29]] > 0).all() and (ref[far[3::31]] > 0).all()
+    np.testing.assert_array_equal(act, ref)
+    assert np.abs(vm - sim.vm()).max() <= VM_TOL_FP64
+
+
 def apd90(trace, times):
     """APD90 per beat of one cell's Vm trace: activation at the first step
     with Vm > 0, V_rest = Vm just before it, V_peak the maximum after it;
