@@ -309,6 +309,96 @@ def run_ours(args):
     print(json.dumps(line), flush=True)
 
 
+def _timed_run(e, steps, warmup, world, local):
+    ms, launches, clocks = time_engine(e, steps, warmup, world, local)
+    return max_over_ranks(ms, world, local), launches, clocks
+
+
+def run_shell(args):
+    """Irregular anatomy: the truncated prolate-ellipsoid shell at 0.25 mm
+    (20 paced endocardial sites), FP64 and mixed, and the mixed path's
+    activation-time error against FP64 over the timed steps."""
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from cardioid_b200 import engine, shell
+    t = shell.prolate_shell(dx=args.shell_dx, seed=1234 + rank)
+    rx = (t.cell_type - 100).astype(np.uint8)
+    out, acts = {}, {}
+    for prec in ("fp64", "mixed"):
+        with engine.Engine(DT, precision=prec, device=local) as e:
+            rid = [e.add_reaction(engine.default_params(c, DT)) for c in (0, 1, 2)]
+            tid = e.add_tissue(t, np.array(rid, np.uint8)[rx])
+            ms, launches, clocks = _timed_run(e, args.steps, 3, world, local)
+            acts[prec] = e.read_activation(tid)
+            out[prec] = {"value": world * t.n * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                         "gpu_launches": launches, "clocks": clocks}
+    a, b = acts["fp64"], acts["mixed"]
+    both = (a > 0) & (b > 0)
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "unit": METRIC, "workload": "prolate shell %.3g mm: %d cells on a %dx%dx%d grid, "
+            "20 paced endocardial sites, steps %d (+3 warm-up) at dt %g" % (args.shell_dx, t.n, t.nx, t.ny, t.nz,
+                                                                          args.steps, DT),
+            "n_gpus": world, "fp64": out["fp64"], "mixed": out["mixed"],
+            "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
+            "mixed_vs_fp64": {"activated_fp64": int((a > 0).sum()), "activated_mixed": int((b > 0).sum()),
+                              "activation_max_err_ms": float(np.abs(a[both] - b[both]).max()) if both.any() else None}}),
+            flush=True)
+
+
+def run_batch(args):
+    """Many instances in one engine: a seeded population (4096 cables,
+    sheets and boxes, per-instance cell type, conductance scales and cycle
+    length); sustained cell-steps/s over the timed steps."""
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from cardioid_b200 import engine, population as pop
+    insts = pop.draw(pop.PopulationSpec(n=args.instances), seed=1234)
+    mine = [i for i in insts if i.index % world == rank]
+    out = {}
+    for prec in args.batch_precisions.split(","):
+        with engine.Engine(DT, precision=prec, device=local) as e:
+            rid = [e.add_reaction(engine.default_params(c, DT)) for c in (0, 1, 2)]
+            t0 = time.perf_counter()
+            for inst in mine:
+                t = pop.build(inst)
+                e.add_tissue(t, np.full(t.n, rid[inst.celltype], np.uint8), scales=inst.scales)
+            setup = time.perf_counter() - t0
+            ms, launches, clocks = _timed_run(e, args.steps, 3, world, local)
+            # every rank steps its share; the time is the slowest rank's
+            out[prec] = {"value": pop.total_cells(insts) * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                         "gpu_launches": launches, "setup_s": setup, "clocks": clocks}
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "unit": METRIC, "n_gpus": world,
+                          "workload": "population of %d instances (%d cells), steps %d (+3 warm-up) at dt %g"
+                          % (len(insts), pop.total_cells(insts), args.steps, DT), **out}), flush=True)
+
+
+def run_serve(args):
+    """Serving: Poisson job arrivals, continuous batching in one engine;
+    p50/p99 time-to-result and aggregate cell-steps/s."""
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    from cardioid_b200 import engine, serving
+    spec = serving.JobSpec(rate=args.rate, steps=args.job_steps)
+    jobs = serving.partition(serving.draw_jobs(args.jobs, spec, seed=1234), rank, world)
+    out = {}
+    for prec in ("mixed", "fp64"):
+        with engine.Engine(DT, precision=prec, device=local) as e:
+            rid = [e.add_reaction(engine.default_params(c, DT)) for c in (0, 1, 2)]
+            srv = serving.Server(e, rid, batch=args.serve_batch)
+            res = srv.run(jobs)
+            out[prec] = serving.summary(res, srv.elapsed, srv.cell_steps)
+            out[prec]["rejected"] = len(srv.rejected)
+    if rank == 0:
+        print(json.dumps({"metric": "time-to-result p50/p99 (s), cell-steps/s", "n_gpus": world,
+                          "workload": "%d jobs, Poisson %.3g/s, log-normal sizes (median 2e5, max 3e7 cells), "
+                          "%d steps each at dt %g" % (args.jobs, args.rate, args.job_steps, DT), **out}), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -333,7 +423,15 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["box256", "box128", "box64"], default="box256")
+    ap.add_argument("--config", choices=["box256", "box128", "box64", "shell", "batch4096", "serve"],
+                    default="box256")
+    ap.add_argument("--shell-dx", type=float, default=0.25)
+    ap.add_argument("--instances", type=int, default=4096)
+    ap.add_argument("--batch-precisions", default="mixed,fp64")
+    ap.add_argument("--jobs", type=int, default=200)
+    ap.add_argument("--rate", type=float, default=5.0)
+    ap.add_argument("--job-steps", type=int, default=2500)
+    ap.add_argument("--serve-batch", type=int, default=250)
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--cpu-steps", type=int, default=40)
     ap.add_argument("--no-cpu", action="store_true")
@@ -345,6 +443,12 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == "shell":
+        run_shell(args)
+    elif args.config == "batch4096":
+        run_batch(args)
+    elif args.config == "serve":
+        run_serve(args)
     else:
         run_ours(args)
 

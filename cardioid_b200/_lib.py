@@ -38,7 +38,8 @@ class TT06Params(ctypes.Structure):
 
 class Stimulus(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
-                ("t0", "tf", "period", "duration", "amplitude", "phase", "xMin", "xMax", "yMin", "yMax", "zMin", "zMax")]
+                ("t0", "tf", "period", "duration", "amplitude", "phase", "xMin", "xMax", "yMin", "yMax", "zMin", "zMax")] + \
+        [("mode", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class EngineConfig(ctypes.Structure):
@@ -169,4 +170,5 @@ def to_stimulus(s):
     c.t0, c.tf, c.period, c.duration = s.t0, s.tf, s.period, s.duration
     c.amplitude, c.phase = s.amplitude, s.tStart
     c.xMin, c.xMax, c.yMin, c.yMax, c.zMin, c.zMax = s.xMin, s.xMax, s.yMin, s.yMax, s.zMin, s.zMax
+    c.mode = s.mode
     return c

@@ -340,8 +340,11 @@ cdb_status validate_desc(const Engine& E, const cdb_tissue_desc* t)
       CDB_CHECK(i == 0 || t->gid[i] > t->gid[i - 1], CDB_INVALID_ARG, "gids must be strictly increasing");
     }
   }
-  for (int s = 0; s < t->nStim; ++s)
+  for (int s = 0; s < t->nStim; ++s) {
     CDB_CHECK(t->stim[s].period > 0 && t->stim[s].duration > 0, CDB_INVALID_ARG, "stimulus period and duration must be > 0");
+    CDB_CHECK(t->stim[s].mode == CDB_STIM_BOX || t->stim[s].mode == CDB_STIM_POINT, CDB_INVALID_ARG,
+              "stimulus mode must be CDB_STIM_BOX or CDB_STIM_POINT");
+  }
   return CDB_OK;
 }
 

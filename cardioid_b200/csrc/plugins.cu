@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(128) reaction_calc_kernel(ReactionArgs a, doub
   const int64_t n = a.n;
   const int32_t e = index[i];
   const double V = Vm[e];
-  const BlockScale none{1.f, 1.f, 1.f};
+  const BlockScale none{1.0, 1.0, 1.0};
   if (MIXED) {
     IOMixed io{a.s64 + i, a.s32 + i, n};
     GenericFits fits{a.coef64, a.coef32, &a.sh};

@@ -7,7 +7,8 @@
 // cell, in the order of the reference's omp loop (elec/simulationLoop.cc:183-231):
 //   FGR stencil on Vm(t) (elec/FGRDiffusionOMP.cc:109-131),
 //   BetterTT06 update (elec/BetterTT06.cc:1426-1649),
-//   box stimuli, assigned in order (elec/BoxStimulus.cc:56-64),
+//   stimuli in order: box assigns (elec/BoxStimulus.cc:56-64), point adds
+//   (elec/PointStimulus.cc:26-36),
 //   Vm(t+dt) = Vm + dt (dVmR + dVmD + iStim) (elec/simulationLoop.cc:221-228),
 //   activation time: first post-step time with Vm > 0 (elec/ActivationTimeSensor.cc:99-111),
 //   min/max Vm (elec/MinMaxSensor.cc:44-67) on request.
@@ -232,7 +233,8 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, int t, int lane, co
     const double v = __shfl_sync(0xffffffffu, stimVal, k);
     if (v != 0.0) {
       const cdb_stimulus* bx = a.stims + stim0 + k;
-      if (x > bx->xMin && x < bx->xMax && y > bx->yMin && y < bx->yMax && z > bx->zMin && z < bx->zMax) istim = v;
+      if (x > bx->xMin && x < bx->xMax && y > bx->yMin && y < bx->yMax && z > bx->zMin && z < bx->zMax)
+        istim = bx->mode == CDB_STIM_POINT ? istim + v : v;
     }
   }
   double vnew = 0.0;

@@ -61,7 +61,7 @@ struct FitShape {
 
 // Per-tissue multipliers of the unfitted conductances (drug block).
 struct BlockScale {
-  float g_Kr, g_CaL, g_Na;
+  double g_Kr, g_CaL, g_Na;
 };
 
 // FP64 quotient without the slow-path branch of the IEEE division: the

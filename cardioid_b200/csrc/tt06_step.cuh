@@ -23,7 +23,7 @@ __device__ __forceinline__ double tt06_step(const TT06Scalars& p, const BlockSca
 {
   using C = ConstsD;
 #define FIT(slot, x) fits.template f64<slot>(x)
-  const double gKr = p.g_Kr * (double)blk.g_Kr, gCaL = p.g_CaL * (double)blk.g_CaL, gNa = p.g_Na * (double)blk.g_Na;
+  const double gKr = p.g_Kr * blk.g_Kr, gCaL = p.g_CaL * blk.g_CaL, gNa = p.g_Na * blk.g_Na;
   const double sqrtKo = 2.32379000772445;   // sqrt(5.4) in double
   const double RT = C::R * C::T;
   const double caSR = io.template get<S_Ca_SR>(), caI = io.template get<S_Ca_i>();
@@ -135,7 +135,7 @@ __device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const Blo
   constexpr float KmCa = 1.38f, KmNai = 87.5f, Alpha = 2.5f, Ko = 5.4f, Pkna = 0.03f, Nao = 140.0f;
   constexpr float KmNa = 40.0f;
   constexpr float RT_F = RT / F;
-  const float gKr = (float)p.g_Kr * blk.g_Kr, gCaL = (float)p.g_CaL * blk.g_CaL, gNa = (float)p.g_Na * blk.g_Na;
+  const float gKr = (float)(p.g_Kr * blk.g_Kr), gCaL = (float)(p.g_CaL * blk.g_CaL), gNa = (float)(p.g_Na * blk.g_Na);
   const float Vf = (float)V;
   const double caSRd = io.template get<S_Ca_SR>(), caId = io.template get<S_Ca_i>();
   const double caSSd = io.template get<S_Ca_ss>(), kId = io.template get<S_K_i>();

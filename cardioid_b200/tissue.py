@@ -45,6 +45,8 @@ class BoxStim:
     period: float = 1000.0
     t0: float = -1000.0
     tf: float = 1e30
+    mode: int = 0           # 0: box (assigns), 1: point (adds; see point_stim)
+    cell: int = -1          # point stimuli: the target gid
 
     @property
     def amplitude(self):
@@ -61,6 +63,15 @@ class BoxStim:
     def as_array(self):
         return np.array([self.t0, self.tf, self.period, self.duration, self.amplitude, self.tStart,
                          self.xMin, self.xMax, self.yMin, self.yMax, self.zMin, self.zMax], dtype=np.float64)
+
+
+def point_stim(gid, nx, ny, **pulse):
+    """A PointStimulus (elec/PointStimulus.cc:6-36) at cell gid: adds the
+    pulse to that cell's iStim.  Expressed as the strict box around the
+    cell's tuple, which holds that cell alone."""
+    x, y, z = gid % nx, (gid // nx) % ny, gid // (nx * ny)
+    return BoxStim(xMin=x - 1, xMax=x + 1, yMin=y - 1, yMax=y + 1, zMin=z - 1, zMax=z + 1, mode=1, cell=int(gid),
+                   **pulse)
 
 
 @dataclass
@@ -162,9 +173,15 @@ def reaction_objects_text(fit_names=None):
 
 
 def stimulus_objects_text(stims, prefix="stim"):
-    """STIMULUS objects (method = box) for the reference's stimulusFactory."""
+    """STIMULUS objects (method = box or point) for the reference's
+    stimulusFactory."""
     out = []
     for i, s in enumerate(stims):
+        if s.mode == 1:
+            out.append("%s%d STIMULUS { method = point; cell = %d; vStim = %r; tStart = %r; duration = %r; "
+                       "period = %r; t0 = %r; tf = %r; }" % (prefix, i, s.cell, s.vStim, s.tStart, s.duration,
+                                                             s.period, s.t0, s.tf))
+            continue
         out.append("%s%d STIMULUS { method = box; xMin = %r; xMax = %r; yMin = %r; yMax = %r; zMin = %r; zMax = %r; "
                    "vStim = %r; tStart = %r; duration = %r; period = %r; t0 = %r; tf = %r; }" % (
                        prefix, i, s.xMin, s.xMax, s.yMin, s.yMax, s.zMin, s.zMax, s.vStim, s.tStart,

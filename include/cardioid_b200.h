@@ -61,14 +61,23 @@ typedef struct {
   double celltype, g_CaL, g_K1, g_Kr, g_Ks, g_Na, g_bca, g_bna, g_pCa, g_pK, g_to;
 } cdb_tt06_params;
 
-/* A BoxStimulus with a PeriodicPulse (elec/BoxStimulus.cc:11-70,
- * elec/PeriodicPulse.cc:22-28, elec/Stimulus.hh:21-27): while
- * t0 < time < tf and phase <= time mod period < phase + duration, cells with
- * xMin < x < xMax, yMin < y < yMax, zMin < z < zMax get iStim = amplitude
- * (= -vStim); a later stimulus overwrites an earlier one. */
+/* A stimulus with a PeriodicPulse (elec/PeriodicPulse.cc:22-28,
+ * elec/Stimulus.hh:21-27): on while t0 < time < tf and
+ * phase <= time mod period < phase + duration, for the cells with
+ * xMin < x < xMax, yMin < y < yMax, zMin < z < zMax.  Stimuli apply in list
+ * order to iStim, which starts each step at 0:
+ *   mode CDB_STIM_BOX   — BoxStimulus (elec/BoxStimulus.cc:11-70): iStim =
+ *                         amplitude (= -vStim), overwriting earlier stimuli;
+ *   mode CDB_STIM_POINT — PointStimulus (elec/PointStimulus.cc:26-36):
+ *                         iStim += amplitude; its box is (x-1, x+1) x
+ *                         (y-1, y+1) x (z-1, z+1) around the target cell. */
+#define CDB_STIM_BOX 0
+#define CDB_STIM_POINT 1
 typedef struct {
   double t0, tf, period, duration, amplitude, phase;
   double xMin, xMax, yMin, yMax, zMin, zMax;
+  int32_t mode;
+  int32_t reserved;   /* 0 */
 } cdb_stimulus;
 
 /* ------------------------------------------------------------------ */

@@ -27,7 +27,8 @@ class OpParams(ctypes.Structure):
 
 class OpStim(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in
-                ("t0", "tf", "period", "duration", "amplitude", "phase", "xMin", "xMax", "yMin", "yMax", "zMin", "zMax")]
+                ("t0", "tf", "period", "duration", "amplitude", "phase", "xMin", "xMax", "yMin", "yMax", "zMin", "zMax")] + \
+        [("mode", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 _lib = None
@@ -91,6 +92,7 @@ def to_c_stim(s):
     c.t0, c.tf, c.period, c.duration = s.t0, s.tf, s.period, s.duration
     c.amplitude, c.phase = s.amplitude, s.tStart
     c.xMin, c.xMax, c.yMin, c.yMax, c.zMin, c.zMax = s.xMin, s.xMax, s.yMin, s.yMax, s.zMin, s.zMax
+    c.mode = s.mode
     return c
 
 

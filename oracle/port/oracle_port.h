@@ -11,7 +11,8 @@
  *   - BetterTT06 CPU calc (1 cell)   elec/BetterTT06.cc:1426-1649
  *   - FGR weights                    elec/FGRDiffusionOMP.cc:166-265, elec/FGRUtils.cc:10-148
  *   - FGR stencil                    elec/FGRDiffusionOMP.cc:109-131
- *   - BoxStimulus / PeriodicPulse    elec/BoxStimulus.cc:11-70, elec/PeriodicPulse.cc:22-28,
+ *   - Box/PointStimulus, PeriodicPulse elec/BoxStimulus.cc:11-70, elec/PointStimulus.cc:26-36,
+ *                                    elec/PeriodicPulse.cc:22-28,
  *                                    elec/Stimulus.hh:21-27
  *   - omp-loop integrator            elec/simulationLoop.cc:183-231
  *   - activation-time sensor         elec/ActivationTimeSensor.cc:99-111
@@ -68,6 +69,9 @@ typedef struct {
    double t0, tf;                       /* Stimulus on while t0 < time < tf */
    double period, duration, amplitude, phase;  /* PeriodicPulse */
    double xMin, xMax, yMin, yMax, zMin, zMax;  /* strict box on the global tuple */
+   int mode;      /* 0: BoxStimulus assigns (elec/BoxStimulus.cc:56-64);
+                     1: PointStimulus adds (elec/PointStimulus.cc:26-36) */
+   int reserved;
 } op_stim_t;
 
 typedef struct op_sim op_sim_t;

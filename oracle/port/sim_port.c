@@ -217,7 +217,7 @@ void op_sim_step(op_sim_t* s, int nSteps)
             int x = (int)(s->gid[i] % s->nx), y = (int)((s->gid[i] / s->nx) % s->ny),
                 z = (int)(s->gid[i] / s->nx / s->ny);
             if (x > p->xMin && x < p->xMax && y > p->yMin && y < p->yMax && z > p->zMin && z < p->zMax)
-               s->iStim[i] = value;
+               s->iStim[i] = p->mode ? s->iStim[i] + value : value;
          }
       }
       /* Cells are independent within each phase, so threading the loops

@@ -205,6 +205,30 @@ def test_activation_after_host_vm_writes(cdb_lib, oracle_port, fits002, graphs):
     assert np.abs(vm - sim.vm()).max() <= VM_TOL_FP64
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_point_and_box_stimuli_match_oracle(cdb_lib, oracle_port, fits002, precision):
+    """Point stimuli add, box stimuli assign, in list order (the port is
+    pinned to the reference on this tissue by test_oracle)."""
+    from test_oracle import _point_stim_tissue
+    t = _point_stim_tissue()
+    rx = _reaction_ids(t)
+    sim = oracle_port.PortSim(t, fits002, rx, DT)
+    sim.step(400)
+    with _engine(fits002, precision=precision) as e:
+        tid = e.add_tissue(t, rx)
+        e.step(400)
+        vm = e.read_vm(tid)
+        act = e.read_activation(tid)
+    ref_act = sim.activation()
+    if precision == "fp64":
+        assert np.abs(vm - sim.vm()).max() <= VM_TOL_FP64
+        np.testing.assert_array_equal(act, ref_act)
+    else:
+        both = (act > 0) & (ref_act > 0)
+        assert (both == (ref_act > 0)).all()
+        assert np.abs(act[both] - ref_act[both]).max() <= ACT_TOL_MIXED
+
+
 def apd90(trace, times):
     """APD90 per beat of one cell's Vm trace: activation at the first step
     with Vm > 0, V_rest = Vm just before it, V_peak the maximum after it;

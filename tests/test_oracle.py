@@ -139,6 +139,51 @@ def test_port_masked_tissue_vs_reference_build(oracle_port, fits002):
     np.testing.assert_array_equal(d2, d1)
 
 
+def _point_stim_tissue():
+    """A masked 9x8x6 box with box and point stimuli in an order that
+    exercises assign-then-add, add-then-assign and a point on a non-tissue
+    voxel (which the reference ignores)."""
+    from cardioid_b200 import tissue
+    full = tissue.box(9, 8, 6, dx=0.2, seed=21)
+    x, y, z = full.tuples()
+    keep = ~((x == 4) & (y == 4) & (z == 3))
+    pulse = dict(vStim=-30.0, duration=1.0, period=3.0)
+    face = tissue.BoxStim(xMin=-1, xMax=1, vStim=-52.0, duration=1.0, period=1000.0)
+    stims = [
+        tissue.point_stim(0 + 9 * (2 + 8 * 1), 9, 8, tStart=0.0, **pulse),   # on the face, then overwritten
+        face,
+        tissue.point_stim(0 + 9 * (3 + 8 * 2), 9, 8, tStart=0.0, **pulse),   # on the face: adds to it
+        tissue.point_stim(6 + 9 * (5 + 8 * 4), 9, 8, tStart=0.4, **pulse),   # interior, later phase
+        tissue.point_stim(4 + 9 * (4 + 8 * 3), 9, 8, tStart=0.0, **pulse),   # removed voxel: no cell
+    ]
+    return tissue.Tissue(full.nx, full.ny, full.nz, full.dx, full.dy, full.dz, full.gid[keep], full.cell_type[keep],
+                         full.sigma[keep], full.vm0[keep], stims)
+
+
+@pytest.mark.skipif(not _ref_built(), reason="oracle/_ref not built")
+def test_port_point_stimuli_vs_reference_build(oracle_port, fits002):
+    """PointStimulus adds its pulse to one cell, BoxStimulus assigns, in
+    list order: port and reference agree bit for bit over 250 steps."""
+    from golden.make_golden import reference_sim
+    t = _point_stim_tissue()
+    ref = reference_sim(t)
+    ref.set_vm(t.vm0)
+    sim = oracle_port.PortSim(t, fits002, (t.cell_type - 100).astype(np.uint8), 0.02)
+    ref.step(1)
+    sim.step(1)
+    _, _, s_ref = ref.dvm()
+    _, _, s_port = sim.dvm()
+    np.testing.assert_array_equal(s_port, s_ref)
+    cell = {int(g): i for i, g in enumerate(t.gid)}
+    assert s_port[cell[9 * (2 + 8 * 1)]] == 52.0            # assigned over the earlier point
+    assert s_port[cell[9 * (3 + 8 * 2)]] == 52.0 + 30.0     # point after the box adds
+    assert s_port[cell[6 + 9 * (5 + 8 * 4)]] == 0.0          # not yet on (tStart 0.4)
+    ref.step(249)
+    sim.step(249)
+    np.testing.assert_array_equal(sim.vm(), ref.vm())
+    np.testing.assert_array_equal(sim.activation(), ref.activation())
+
+
 def test_fit_eval_port_matches_python(oracle_port, fits002):
     """Interpolation::eval restated in C and in numpy agree bit for bit."""
     x = np.linspace(-100, 100, 37)
