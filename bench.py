@@ -28,8 +28,9 @@ DT = 0.02
 METRIC = "cell-steps/s"
 # algorithmic bytes per cell-step of one fused step (compulsory HBM traffic):
 # Vm read+write 16 B; state FP64 18x8x2 = 288 B, mixed 5x8x2 + 13x4x2 = 184 B;
-# stencil weights FP64 19x8 = 152 B, mixed 18x4 = 72 B; reaction byte 1 B.
-ALGO_BYTES = {"fp64": 16 + 288 + 152 + 1, "mixed": 16 + 184 + 72 + 1}
+# stencil weights FP64 19x8 = 152 B, mixed 18x4 = 72 B; the cell's voxel
+# offset 4 B (the reaction type is per warp tile, not per cell).
+ALGO_BYTES = {"fp64": 16 + 288 + 152 + 4, "mixed": 16 + 184 + 72 + 4}
 CPU_SAMPLE = (64, 64, 32)     # cells per CPU worker process
 
 

@@ -10,15 +10,18 @@
 //   vm[2]      padded Vm blocks (halo of one voxel, zero, never written)
 //              in x-fastest order; only dimensions longer than one voxel
 //              are padded (a cable is nx+2 long, a sheet (nx+2)(ny+2));
-//   s64, s32   state, structure of arrays with pitch n: FP64 path 18 rows
-//              of double; mixed path 5 rows of double (Ca_SR Ca_i Ca_ss K_i
+//   slots      cells grouped by reaction type, each group padded to whole
+//              32-slot blocks (slot map: cell -> slot);
+//   s64, s32   state, AoSoA blocks of 32 slots: FP64 path 18 rows of
+//              double; mixed path 5 rows of double (Ca_SR Ca_i Ca_ss K_i
 //              Na_i) and 13 of float (R_prime and the 12 gates);
-//   w          stencil weights, rows x n (FP64: A0 and the class's nodes in
+//   w          stencil weights, AoSoA (FP64: A0 and the class's nodes in
 //              double; mixed: the class's nodes without A0 in float);
+//   vrel       per slot, int32 voxel offset from its block's first voxel;
 //   voxel      (masked tissues only) int64 padded-voxel index per cell;
-//   act        activation time per cell.
-// A warp-tile table, grouped by reaction type, maps each warp to up to 32
-// consecutive cells of one tissue and one reaction type (step_kernel.cuh).
+//   act        activation time per slot.
+// A warp-tile table, grouped by reaction type, maps each warp to one block
+// (step_kernel.cuh).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -68,6 +71,9 @@ struct HostTissue {
   std::vector<cdb_stimulus> stims;
   DeviceBuffer vm0, vm1, s64, s32, w, voxel, act, minmax;
   std::vector<WarpTile> tiles[CDB_MAX_REACTION_TYPES];   // by slot; .tissue set at rebuild
+  int64_t nSlots = 0;               // AoSoA slots (cells plus padding)
+  std::vector<int64_t> slot;        // slot of every cell
+  DeviceBuffer slotMap, vrel;       // device copies: cell -> slot; per-slot voxel offsets
   int64_t steps = 0;       // steps taken
   int parity = 0;
   int64_t n = 0;
@@ -360,18 +366,85 @@ int64_t padded_voxels(int nx, int ny, int nz, int cls, int64_t* px, int64_t* pxy
   return Px * Py * Pz;
 }
 
+// Slots per reaction type of a tissue: its cells grouped by type, each
+// group rounded up to whole 32-slot blocks.
+int64_t count_slots(int64_t n, const uint8_t* reaction, const int* slots, int64_t count[CDB_MAX_REACTION_TYPES])
+{
+  for (int k = 0; k < CDB_MAX_REACTION_TYPES; ++k) count[k] = 0;
+  for (int64_t c = 0; c < n; ++c) ++count[slots[reaction[c]]];
+  int64_t total = 0;
+  for (int k = 0; k < CDB_MAX_REACTION_TYPES; ++k) total += (count[k] + kBlk - 1) / kBlk * kBlk;
+  return total;
+}
+
+// The slot layout and warp tiles of a tissue.  Cells are grouped by reaction
+// type (constant-memory slot, ascending), in cell order within a type, each
+// group starting on a 32-slot block, so every AoSoA block holds one type and
+// every warp tile is full but the last of its type (the per-type cell
+// grouping of ReactionManager::create, elec/ReactionManager.cc:74-371).
+// Fills h.slot, h.tiles, h.nSlots and vrel (per slot: voxel offset from its
+// tile's first voxel; 0 for padding).
+cdb_status build_layout(HostTissue& h, const int64_t* gid, const uint8_t* reaction, const int* slots,
+                        const cdb_stimulus* stim, int nStim, std::vector<int32_t>& vrel)
+{
+  const TissueDev& d = h.dev;
+  const int64_t n = h.n;
+  int64_t count[CDB_MAX_REACTION_TYPES], start[CDB_MAX_REACTION_TYPES], next[CDB_MAX_REACTION_TYPES];
+  h.nSlots = count_slots(n, reaction, slots, count);
+  int64_t total = 0;
+  for (int k = 0; k < CDB_MAX_REACTION_TYPES; ++k) {
+    start[k] = next[k] = total;
+    total += (count[k] + kBlk - 1) / kBlk * kBlk;
+  }
+  h.slot.resize(n);
+  std::vector<int64_t> voxOf(h.nSlots, 0);
+  std::vector<unsigned> mask(h.nSlots / kBlk, 0u);
+  for (int64_t c = 0; c < n; ++c) {
+    const int64_t i = next[slots[reaction[c]]]++;
+    h.slot[c] = i;
+    const int64_t g = gid ? gid[c] : c;
+    const int x = (int)(g % h.nx);
+    const int64_t yz = g / h.nx;
+    const int y = (int)(yz % h.ny), z = (int)(yz / h.ny);
+    voxOf[i] = (int64_t)(x + 1) + d.px * (int64_t)(y + d.py0) + d.pxy * (int64_t)(z + d.pz0);
+    for (int k = 0; k < nStim; ++k) {
+      const cdb_stimulus& b = stim[k];
+      if (x > b.xMin && x < b.xMax && y > b.yMin && y < b.yMax && z > b.zMin && z < b.zMax) mask[i / kBlk] |= 1u << k;
+    }
+  }
+  vrel.assign(h.nSlots, 0);
+  for (auto& v : h.tiles) v.clear();
+  for (int k = 0; k < CDB_MAX_REACTION_TYPES; ++k)
+    for (int64_t f = start[k]; f < start[k] + count[k]; f += kBlk) {
+      WarpTile tl{};
+      tl.first = f;
+      tl.count = (int)std::min<int64_t>(kBlk, start[k] + count[k] - f);
+      tl.vox0 = voxOf[f];
+      tl.stimMask = mask[f / kBlk];
+      for (int l = 0; l < tl.count; ++l) {
+        const int64_t r = voxOf[f + l] - tl.vox0;
+        CDB_CHECK(r >= INT32_MIN && r <= INT32_MAX, CDB_INVALID_ARG,
+                  "grid too large: 32 consecutive cells of one type span more than 2^31 voxels");
+        vrel[f + l] = (int32_t)r;
+      }
+      h.tiles[k].push_back(tl);
+    }
+  return CDB_OK;
+}
+
 int64_t tissue_bytes(const Engine& E, const cdb_tissue_desc* t)
 {
   const bool masked = t->gid && t->nCells != (int64_t)t->nx * t->ny * t->nz;
   const int cls = tissue_class(t->nx, t->ny, t->nz, masked);
   const int64_t vox = padded_voxels(t->nx, t->ny, t->nz, cls, nullptr, nullptr, nullptr, nullptr);
   const int64_t n = t->nCells;
-  const int64_t nPad = (n + kBlk - 1) / kBlk * kBlk;
+  int64_t count[CDB_MAX_REACTION_TYPES];
+  const int64_t nSlots = count_slots(n, t->reaction, E.slots, count);
   const bool mixed = E.cfg.precision == CDB_MIXED;
   int64_t b = 2 * vox * 8;                                                   // Vm blocks
-  b += mixed ? nPad * (kRowsMixed64 * 8 + kRowsMixed32 * 4) : nPad * kRows64 * 8;   // state
-  b += nPad * weight_rows(cls, mixed) * (mixed ? 4 : 8);                     // weights
-  b += n * 8 + (masked ? n * 8 : 0) + 64;                                   // act, voxel
+  b += mixed ? nSlots * (kRowsMixed64 * 8 + kRowsMixed32 * 4) : nSlots * kRows64 * 8;   // state
+  b += nSlots * weight_rows(cls, mixed) * (mixed ? 4 : 8);                   // weights
+  b += nSlots * (8 + 4) + n * 8 + (masked ? n * 8 : 0) + 64;                 // act, vrel, slot map, voxel
   return b;
 }
 
@@ -499,37 +572,6 @@ cdb_status cdb_engine_free_bytes(cdb_engine* e, int64_t* freeBytes, int64_t* tot
   return CDB_OK;
 }
 
-// A tissue's warp tiles, by constant-memory slot: runs of cells that share
-// a reaction type, lie in one 32-cell AoSoA block and occupy consecutive
-// voxels of one grid row (gid = x + nx (y + ny z); NULL gid = all cells).
-void build_tiles(HostTissue& h, const int64_t* gid, const uint8_t* reaction, const int* slots)
-{
-  const TissueDev& d = h.dev;
-  for (auto& v : h.tiles) v.clear();
-  int64_t f = 0;
-  while (f < h.n) {
-    const int slot = slots[reaction[f]];
-    const int64_t g0 = gid ? gid[f] : f;
-    const int x0 = (int)(g0 % h.nx);
-    const int64_t yz = g0 / h.nx;
-    const int y = (int)(yz % h.ny), z = (int)(yz / h.ny);
-    const int64_t blockEnd = (f / kBlk + 1) * kBlk;
-    int64_t e = f + 1;
-    while (e < h.n && e < blockEnd && slots[reaction[e]] == slot && x0 + (e - f) < h.nx &&
-           (gid ? gid[e] : e) == g0 + (e - f))
-      ++e;
-    WarpTile tl{};
-    tl.first = f;
-    tl.count = (int)(e - f);
-    tl.vox0 = (int64_t)(x0 + 1) + d.px * (int64_t)(y + d.py0) + d.pxy * (int64_t)(z + d.pz0);
-    tl.x0 = x0;
-    tl.y = y;
-    tl.z = z;
-    h.tiles[slot].push_back(tl);
-    f = e;
-  }
-}
-
 cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_t* id)
 {
   CDB_CHECK(e && id, CDB_INVALID_ARG, "null argument");
@@ -560,18 +602,27 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
   CDB_CUDA(h->vm1.alloc(vox * 8));
   CDB_CUDA(cudaMemsetAsync(h->vm0.p, 0, vox * 8, s));
   CDB_CUDA(cudaMemsetAsync(h->vm1.p, 0, vox * 8, s));
-  // AoSoA arrays cover whole 32-cell blocks
-  const int64_t nPad = (n + kBlk - 1) / kBlk * kBlk;
+  // slots grouped by reaction type; AoSoA arrays cover whole 32-slot blocks
+  std::vector<int32_t> vrel;
+  {
+    const cdb_status ls = build_layout(*h, t->gid, t->reaction, E.slots, t->stim, t->nStim, vrel);
+    if (ls != CDB_OK) return ls;
+  }
+  const int64_t nSlots = h->nSlots;
   if (mixed) {
-    CDB_CUDA(h->s64.alloc(nPad * kRowsMixed64 * 8));
-    CDB_CUDA(h->s32.alloc(nPad * kRowsMixed32 * 4));
+    CDB_CUDA(h->s64.alloc(nSlots * kRowsMixed64 * 8));
+    CDB_CUDA(h->s32.alloc(nSlots * kRowsMixed32 * 4));
   } else {
-    CDB_CUDA(h->s64.alloc(nPad * kRows64 * 8));
+    CDB_CUDA(h->s64.alloc(nSlots * kRows64 * 8));
   }
   const int wrows = weight_rows(cls, mixed);
-  CDB_CUDA(h->w.alloc(nPad * wrows * (mixed ? 4 : 8)));
-  CDB_CUDA(cudaMemsetAsync(h->w.p, 0, nPad * wrows * (mixed ? 4 : 8), s));
-  CDB_CUDA(h->act.alloc(n * 8));
+  CDB_CUDA(h->w.alloc(nSlots * wrows * (mixed ? 4 : 8)));
+  CDB_CUDA(cudaMemsetAsync(h->w.p, 0, nSlots * wrows * (mixed ? 4 : 8), s));
+  CDB_CUDA(h->act.alloc(nSlots * 8));
+  CDB_CUDA(h->vrel.alloc(nSlots * 4));
+  CDB_CUDA(h->slotMap.alloc(n * 8));
+  CDB_CUDA(cudaMemcpyAsync(h->vrel.p, vrel.data(), nSlots * 4, cudaMemcpyHostToDevice, s));
+  CDB_CUDA(cudaMemcpyAsync(h->slotMap.p, h->slot.data(), n * 8, cudaMemcpyHostToDevice, s));
   CDB_CUDA(h->minmax.alloc(16));
   if (masked) CDB_CUDA(h->voxel.alloc(n * 8));
 
@@ -593,7 +644,7 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
                                                             map.as<int64_t>(), cellVoxel.as<int64_t>());
     build_weights_kernel<<<grid_for(n, 128), 128, 0, s>>>(n, map.as<int64_t>(), cellVoxel.as<int64_t>(),
                                                           sig.as<double>(), bx, bxy, t->dx, t->dy, t->dz, cls,
-                                                          mixed ? 1 : 0, h->w.p);
+                                                          mixed ? 1 : 0, h->slotMap.as<int64_t>(), h->w.p);
     E.launches += 2;
     if (masked) {
       // cell voxels in the engine's (class-padded) block; masked tissues are kVolume
@@ -607,7 +658,6 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
       CDB_CUDA(cudaMemcpyAsync(h->voxel.p, v.data(), n * 8, cudaMemcpyHostToDevice, s));
       CDB_CUDA(cudaStreamSynchronize(s));
     }
-    build_tiles(*h, t->gid, t->reaction, E.slots);
     CDB_CUDA(cudaStreamSynchronize(s));
   }
   d.vm[0] = h->vm0.as<double>();
@@ -619,7 +669,8 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
   d.act = h->act.as<double>();
   d.minmax = h->minmax.as<unsigned long long>();
   d.actAll = 1;
-  init_state_kernel<<<grid_for(nPad, 256), 256, 0, s>>>(nPad, d.s64, d.s32, mixed ? 1 : 0, d.act, n);
+  d.vrel = h->vrel.as<int>();
+  init_state_kernel<<<grid_for(nSlots, 256), 256, 0, s>>>(nSlots, d.s64, d.s32, mixed ? 1 : 0, d.act);
   E.launches += 1;
   {
     DeviceBuffer v0;
@@ -734,7 +785,7 @@ cdb_status cdb_engine_read_state(cdb_engine* e, int32_t id, int var, double* hos
   const int64_t n = t->n;
   DeviceBuffer tmp;
   CDB_CUDA(tmp.alloc(n * 8));
-  gather_state_kernel<<<grid_for(n, 256), 256, 0, E.stream>>>(n, t->dev.s64, t->dev.s32,
+  gather_state_kernel<<<grid_for(n, 256), 256, 0, E.stream>>>(n, t->slotMap.as<int64_t>(), t->dev.s64, t->dev.s32,
                                                               E.cfg.precision == CDB_MIXED, var, tmp.as<double>());
   E.launches += 1;
   CDB_CUDA(cudaMemcpyAsync(host, tmp.p, n * 8, cudaMemcpyDeviceToHost, E.stream));
@@ -755,7 +806,7 @@ cdb_status cdb_engine_write_state(cdb_engine* e, int32_t id, int var, const doub
   DeviceBuffer tmp;
   CDB_CUDA(tmp.alloc(n * 8));
   CDB_CUDA(cudaMemcpyAsync(tmp.p, host, n * 8, cudaMemcpyHostToDevice, E.stream));
-  scatter_state_kernel<<<grid_for(n, 256), 256, 0, E.stream>>>(n, t->dev.s64, t->dev.s32,
+  scatter_state_kernel<<<grid_for(n, 256), 256, 0, E.stream>>>(n, t->slotMap.as<int64_t>(), t->dev.s64, t->dev.s32,
                                                                E.cfg.precision == CDB_MIXED, var, tmp.as<double>());
   E.launches += 1;
   CDB_CUDA(cudaStreamSynchronize(E.stream));
@@ -770,7 +821,13 @@ cdb_status cdb_engine_read_activation(cdb_engine* e, int32_t id, double* host)
   Engine& E = e->e;
   CDB_CUDA(cudaSetDevice(E.cfg.device));
   CDB_CUDA(cudaStreamSynchronize(E.stream));
-  CDB_CUDA(cudaMemcpy(host, t->dev.act, t->n * 8, cudaMemcpyDeviceToHost));
+  DeviceBuffer tmp;
+  CDB_CUDA(tmp.alloc(t->n * 8));
+  gather_slots_kernel<<<grid_for(t->n, 256), 256, 0, E.stream>>>(t->n, t->slotMap.as<int64_t>(), t->dev.act,
+                                                                 tmp.as<double>());
+  E.launches += 1;
+  CDB_CUDA(cudaMemcpyAsync(host, tmp.p, t->n * 8, cudaMemcpyDeviceToHost, E.stream));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
   return CDB_OK;
 }
 
@@ -802,24 +859,23 @@ cdb_status cdb_engine_read_weights(cdb_engine* e, int32_t id, double* host19)
   const int rows = class_rows(cls);
   const bool mixed = E.cfg.precision == CDB_MIXED;
   std::vector<double> out(n * 19, 0.0);
-  const int64_t nPad = (n + kBlk - 1) / kBlk * kBlk;
   if (mixed) {
-    std::vector<float> w((size_t)nPad * (rows - 1));
+    std::vector<float> w((size_t)t->nSlots * (rows - 1));
     CDB_CUDA(cudaMemcpy(w.data(), t->dev.w, w.size() * 4, cudaMemcpyDeviceToHost));
     for (int64_t i = 0; i < n; ++i) {
       double a0 = 0;
       for (int r = 1; r < rows; ++r) {
-        const float v = w[aosoa(i, rows - 1, r - 1)];
+        const float v = w[aosoa(t->slot[i], rows - 1, r - 1)];
         out[i * 19 + class_node(cls, r)] = v;
         a0 -= v;
       }
       out[i * 19] = a0;
     }
   } else {
-    std::vector<double> w((size_t)nPad * rows);
+    std::vector<double> w((size_t)t->nSlots * rows);
     CDB_CUDA(cudaMemcpy(w.data(), t->dev.w, w.size() * 8, cudaMemcpyDeviceToHost));
     for (int64_t i = 0; i < n; ++i)
-      for (int r = 0; r < rows; ++r) out[i * 19 + class_node(cls, r)] = w[aosoa(i, rows, r)];
+      for (int r = 0; r < rows; ++r) out[i * 19 + class_node(cls, r)] = w[aosoa(t->slot[i], rows, r)];
   }
   std::memcpy(host19, out.data(), out.size() * 8);
   return CDB_OK;

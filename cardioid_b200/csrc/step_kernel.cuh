@@ -39,8 +39,9 @@ struct TissueDev {
   double* s64;            // AoSoA: FP64 [nb][18][32]; mixed [nb][5][32]
   float* s32;             // AoSoA: mixed [nb][13][32]
   const void* w;          // AoSoA: FP64 [nb][rows][32] doubles; mixed [nb][rows-1][32] floats
-  const int64_t* voxel;
-  double* act;
+  const int64_t* voxel;    // masked tissues: padded voxel of every cell, in cell order
+  const int* vrel;         // per slot: voxel offset from its tile's vox0
+  double* act;             // per slot
   int64_t n;
   int64_t px, pxy;        // padded strides
   int nx, ny, nz;
@@ -55,15 +56,17 @@ struct TissueDev {
   unsigned long long* minmax;   // 2 slots
 };
 
-// A warp tile: up to 32 cells of one tissue that share a reaction type, lie
-// in one 32-cell AoSoA block and occupy consecutive voxels of one grid row,
-// so lane l's cell is first + l, its voxel vox0 + l, its x x0 + l.
+// A warp tile: one 32-slot AoSoA block of one tissue, whose slots hold
+// cells of one reaction type (count of them, the rest are padding).  Lane l
+// works on slot first + l, whose voxel in the padded Vm block is vox0 plus
+// the slot's offset (TissueDev::vrel).  Bit k of stimMask is set when
+// stimulus k's box holds a cell of the tile.
 struct WarpTile {
   int tissue;
   int count;
   int64_t first;
-  int64_t vox0;           // padded-block voxel of the first cell
-  int x0, y, z;           // grid coordinates of the first cell
+  int64_t vox0;
+  unsigned stimMask;
   int pad;
 };
 
@@ -92,11 +95,16 @@ __host__ __device__ constexpr int weight_rows(int cls, bool mixed) { return mixe
 
 // Shared-memory staging per warp and buffer: the mixed path stages its state
 // block and its weight block (up to 18 float rows), the FP64 path its state
-// block (its weights are read directly).
+// block (its weights are read directly); both stage the slots' voxel offsets.
+template <bool MIXED>
+__host__ __device__ constexpr int vrel_offset()
+{
+  return MIXED ? (kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4 + 18 * kBlk * 4) : kRows64 * kBlk * 8;
+}
 template <bool MIXED>
 __host__ __device__ constexpr int stage_bytes()
 {
-  return MIXED ? (kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4 + 18 * kBlk * 4) : kRows64 * kBlk * 8;
+  return vrel_offset<MIXED>() + kBlk * 4;
 }
 
 __device__ __forceinline__ double pulse_value(const cdb_stimulus& s, double time)
@@ -203,6 +211,7 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, int t, int lane, u
   } else {
     warp_copy(buf, (const unsigned char*)(Tp->s64 + b * kRows64 * kBlk), kRows64 * kBlk * 8, lane);
   }
+  warp_copy(buf + vrel_offset<MIXED>(), (const unsigned char*)(Tp->vrel + b * kBlk), kBlk * 4, lane);
 }
 
 // One tile.  With `staged` the tile's state (and mixed weights) are read
@@ -216,25 +225,29 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, int t, int lane, co
   const int64_t lstep = Tp->step0 + a.k;
   const double time = a.times[lstep];
   const double tnext = a.times[lstep + 1];
-  const int nstim = Tp->nstim;
-  const int stim0 = Tp->stim0;
-  // lane s holds stimulus s's value at this time
-  const double stimVal = lane < nstim ? pulse_value(a.stims[stim0 + lane], time) : 0.0;
   const bool active = lane < tile.count;
   // lanes past the tile's end stand in for its first cell until the end
   const int l = active ? lane : 0;
   const int64_t i = tile.first + l;
-  const int64_t vox = tile.vox0 + l;
-  const int x = tile.x0 + l, y = tile.y, z = tile.z;
+  const int rel = staged ? ((const int*)(buf + vrel_offset<MIXED>()))[l] : Tp->vrel[i];
+  const int64_t vox = tile.vox0 + rel;
   const int64_t px = Tp->px, pxy = Tp->pxy;
-  // iStim = 0, then every stimulus that is on assigns its value inside its box
+  // iStim = 0, then the stimuli whose boxes hold a cell of the tile, in order
   double istim = 0.0;
-  for (int k = 0; k < nstim; ++k) {
-    const double v = __shfl_sync(0xffffffffu, stimVal, k);
-    if (v != 0.0) {
-      const cdb_stimulus* bx = a.stims + stim0 + k;
-      if (x > bx->xMin && x < bx->xMax && y > bx->yMin && y < bx->yMax && z > bx->zMin && z < bx->zMax)
-        istim = bx->mode == CDB_STIM_POINT ? istim + v : v;
+  if (tile.stimMask) {
+    const int stim0 = Tp->stim0;
+    // lane s holds stimulus s's value at this time
+    const double stimVal = lane < Tp->nstim ? pulse_value(a.stims[stim0 + lane], time) : 0.0;
+    const int64_t zz = vox / pxy, rem = vox - zz * pxy, yy = rem / px;
+    const int x = (int)(rem - yy * px) - 1, y = (int)yy - Tp->py0, z = (int)zz - Tp->pz0;
+    for (unsigned m = tile.stimMask; m; m &= m - 1) {
+      const int k = __ffs(m) - 1;
+      const double v = __shfl_sync(0xffffffffu, stimVal, k);
+      if (v != 0.0) {
+        const cdb_stimulus* bx = a.stims + stim0 + k;
+        if (x > bx->xMin && x < bx->xMax && y > bx->yMin && y < bx->yMax && z > bx->zMin && z < bx->zMax)
+          istim = bx->mode == CDB_STIM_POINT ? istim + v : v;
+      }
     }
   }
   double vnew = 0.0;
@@ -443,24 +456,27 @@ __global__ void build_voxel_map_kernel(int64_t n, const int64_t* __restrict__ gi
   cellVoxel[i] = v;
 }
 
-// Weights of every cell (fgr_cell_weights), written AoSoA in the tissue's
-// class layout: FP64 rows = A0 then the class nodes; mixed rows = class nodes.
+// Weights of every cell (fgr_cell_weights), written AoSoA at the cell's
+// slot in the tissue's class layout: FP64 rows = A0 then the class nodes;
+// mixed rows = class nodes.
 __global__ void build_weights_kernel(int64_t n, const int64_t* __restrict__ map, const int64_t* __restrict__ cellVoxel,
                                      const double* __restrict__ sigma6, int64_t bx, int64_t bxy, double hx, double hy,
-                                     double hz, int cls, int mixed, void* __restrict__ wout)
+                                     double hz, int cls, int mixed, const int64_t* __restrict__ slot,
+                                     void* __restrict__ wout)
 {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int64_t v = cellVoxel[i];
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int64_t v = cellVoxel[c];
+  const int64_t i = slot[c];
   int tissue[19];
   int64_t nbrCell[19];
   for (int k = 0; k < 19; ++k) {
-    const int64_t c = map[v + node_dx(k) + bx * node_dy(k) + bxy * node_dz(k)];
-    nbrCell[k] = c;
-    tissue[k] = c >= 0;
+    const int64_t nb = map[v + node_dx(k) + bx * node_dy(k) + bxy * node_dz(k)];
+    nbrCell[k] = nb;
+    tissue[k] = nb >= 0;
   }
   double W[19];
-  fgr_cell_weights(tissue, [&](int k, int c) { return sigma6[6 * nbrCell[k] + c]; }, hx, hy, hz, W);
+  fgr_cell_weights(tissue, [&](int k, int e) { return sigma6[6 * nbrCell[k] + e]; }, hx, hy, hz, W);
   const int rows = class_rows(cls);
   if (mixed) {
     float* w = (float*)wout;
@@ -500,32 +516,43 @@ __global__ void gather_vm_kernel(int64_t n, const double* __restrict__ blk, doub
   if (i < n) dst[i] = blk[cell_voxel(i, voxel, nx, ny, px, pxy, py0, pz0)];
 }
 
-// Row var of the AoSoA state to / from a cell-order array of doubles.
-__global__ void gather_state_kernel(int64_t n, const double* __restrict__ s64, const float* __restrict__ s32,
-                                    int mixed, int var, double* __restrict__ dst)
+// Row var of the AoSoA state to / from a cell-order array of doubles
+// (slot[c]: the slot of cell c).
+__global__ void gather_state_kernel(int64_t n, const int64_t* __restrict__ slot, const double* __restrict__ s64,
+                                    const float* __restrict__ s32, int mixed, int var, double* __restrict__ dst)
 {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (!mixed) dst[i] = s64[aosoa(i, kRows64, var)];
-  else if (var < kRowsMixed64) dst[i] = s64[aosoa(i, kRowsMixed64, var)];
-  else dst[i] = (double)s32[aosoa(i, kRowsMixed32, var - kRowsMixed64)];
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int64_t i = slot[c];
+  if (!mixed) dst[c] = s64[aosoa(i, kRows64, var)];
+  else if (var < kRowsMixed64) dst[c] = s64[aosoa(i, kRowsMixed64, var)];
+  else dst[c] = (double)s32[aosoa(i, kRowsMixed32, var - kRowsMixed64)];
 }
 
-__global__ void scatter_state_kernel(int64_t n, double* __restrict__ s64, float* __restrict__ s32, int mixed, int var,
-                                     const double* __restrict__ src)
+__global__ void scatter_state_kernel(int64_t n, const int64_t* __restrict__ slot, double* __restrict__ s64,
+                                     float* __restrict__ s32, int mixed, int var, const double* __restrict__ src)
 {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (!mixed) s64[aosoa(i, kRows64, var)] = src[i];
-  else if (var < kRowsMixed64) s64[aosoa(i, kRowsMixed64, var)] = src[i];
-  else s32[aosoa(i, kRowsMixed32, var - kRowsMixed64)] = (float)src[i];
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int64_t i = slot[c];
+  if (!mixed) s64[aosoa(i, kRows64, var)] = src[c];
+  else if (var < kRowsMixed64) s64[aosoa(i, kRowsMixed64, var)] = src[c];
+  else s32[aosoa(i, kRowsMixed32, var - kRowsMixed64)] = (float)src[c];
 }
 
-// Initial state of every cell of the padded block count (pad cells too).
-__global__ void init_state_kernel(int64_t nPad, double* s64, float* s32, int mixed, double* act, int64_t n)
+// Per-slot values (activation times) to cell order.
+__global__ void gather_slots_kernel(int64_t n, const int64_t* __restrict__ slot, const double* __restrict__ src,
+                                    double* __restrict__ dst)
+{
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c < n) dst[c] = src[slot[c]];
+}
+
+// Initial state and activation time of every slot (padding slots too).
+__global__ void init_state_kernel(int64_t nSlots, double* s64, float* s32, int mixed, double* act)
 {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= nPad) return;
+  if (i >= nSlots) return;
   if (mixed) {
     for (int k = 0; k < kRowsMixed64; ++k) s64[aosoa(i, kRowsMixed64, k)] = tt06_initial_state(k);
     for (int k = kRowsMixed64; k < kNumStates; ++k)
@@ -533,7 +560,7 @@ __global__ void init_state_kernel(int64_t nPad, double* s64, float* s32, int mix
   } else {
     for (int k = 0; k < kNumStates; ++k) s64[aosoa(i, kRows64, k)] = tt06_initial_state(k);
   }
-  if (i < n) act[i] = -1.0;
+  act[i] = -1.0;
 }
 
 __global__ void fill_kernel(int64_t n, double* p, double v)
