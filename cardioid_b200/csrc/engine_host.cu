@@ -75,6 +75,7 @@ struct HostTissue {
   std::vector<int64_t> slot;        // slot of every cell
   DeviceBuffer slotMap, vrel;       // device copies: cell -> slot; per-slot voxel offsets
   int64_t steps = 0;       // steps taken
+  int clock = 0;           // its time sequence (Engine::clocks)
   int parity = 0;
   int64_t n = 0;
   int nx = 0, ny = 0, nz = 0;
@@ -117,7 +118,17 @@ struct Engine {
   bool dirty = true;
   // tables
   DeviceBuffer dTissues, dTiles, dStims, dTimes, dStage;
-  std::vector<double> times{0.0};
+  // Time sequences: clock c gives time[s] = clocks[c].times[s - base] for
+  // step s >= base, accumulated as time += dt like the reference
+  // (elec/simulationLoop.cc:230).  Clock 0 starts at step 0, time 0; a
+  // restarted tissue (cdb_engine_set_clock) may need its own.  dTimes holds
+  // all of them back to back, clock c from offset clocks[c].off.
+  struct Clock {
+    int64_t base;
+    std::vector<double> times;
+    int64_t off;
+  };
+  std::vector<Clock> clocks{Clock{0, {0.0}, 0}};
   std::vector<int> order;         // tissue ids in table order
   int64_t nTiles = 0;
   std::vector<std::pair<int, std::pair<int, int>>> slotTiles;   // slot -> (first tile, tile count)
@@ -148,20 +159,42 @@ struct Engine {
     for (int t = 0; t < nTypes; ++t) release_slot(cfg.device, slots[t]);
   }
 
-  cdb_status ensure_times(int64_t upto)
+  // Every tissue's clock covers `extra` steps past its current step (+1 for
+  // the time after the last of them); re-uploads dTimes when a clock grew.
+  cdb_status ensure_times(int64_t extra)
   {
-    if ((int64_t)times.size() > upto) {
-      if (dTimes.bytes >= times.size() * sizeof(double)) return CDB_OK;
+    std::vector<int64_t> need(clocks.size(), 1);
+    for (auto& kv : tissues) {
+      const Clock& c = clocks[kv.second->clock];
+      need[kv.second->clock] = std::max(need[kv.second->clock], kv.second->steps - c.base + extra + 1);
     }
-    int64_t want = std::max<int64_t>(upto + 1, (int64_t)times.size() * 2);
-    times.reserve(want);
-    while ((int64_t)times.size() < want) times.push_back(times.back() + cfg.dt);
-    // the reference advances time as time += dt (elec/simulationLoop.cc:230)
+    bool grew = dTimes.p == nullptr;
+    for (size_t c = 0; c < clocks.size(); ++c) {
+      std::vector<double>& t = clocks[c].times;
+      if ((int64_t)t.size() >= need[c]) continue;
+      const int64_t want = std::max<int64_t>(need[c], (int64_t)t.size() * 2);
+      t.reserve(want);
+      while ((int64_t)t.size() < want) t.push_back(t.back() + cfg.dt);
+      grew = true;
+    }
+    if (!grew) return CDB_OK;
+    std::vector<double> all;
+    for (Clock& c : clocks) {
+      c.off = (int64_t)all.size();
+      all.insert(all.end(), c.times.begin(), c.times.end());
+    }
     CDB_CUDA(cudaStreamSynchronize(stream));
-    CDB_CUDA(dTimes.alloc(times.size() * sizeof(double)));
-    CDB_CUDA(cudaMemcpy(dTimes.p, times.data(), times.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CDB_CUDA(dTimes.alloc(all.size() * sizeof(double)));
+    CDB_CUDA(cudaMemcpy(dTimes.p, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
     if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    dirty = true;   // tissues' time offsets
     return CDB_OK;
+  }
+
+  double tissue_time(const HostTissue& t) const
+  {
+    const Clock& c = clocks[t.clock];
+    return c.times[t.steps - c.base];
   }
 
   cdb_status rebuild()
@@ -180,6 +213,7 @@ struct Engine {
       stims.insert(stims.end(), t.stims.begin(), t.stims.end());
       t.dev.step0 = t.steps;
       t.dev.parity = t.parity;
+      t.dev.timeOff = clocks[t.clock].off - clocks[t.clock].base;
       const int idx = (int)devs.size();
       devs.push_back(t.dev);
       order.push_back(kv.first);
@@ -267,11 +301,9 @@ struct Engine {
   {
     CDB_CHECK(k >= 0, CDB_INVALID_ARG, "nSteps must be >= 0");
     if (k == 0 || tissues.empty()) return CDB_OK;
-    cdb_status st = rebuild();
+    cdb_status st = ensure_times(k);
     if (st != CDB_OK) return st;
-    int64_t maxStep = 0;
-    for (auto& kv : tissues) maxStep = std::max(maxStep, kv.second->steps);
-    st = ensure_times(maxStep + k + 1);
+    st = rebuild();
     if (st != CDB_OK) return st;
     if (cfg.use_graphs) {
       if (!graph || graphSteps != k || graphMinmax != minmax) {
@@ -728,10 +760,40 @@ cdb_status cdb_engine_tissue_time(cdb_engine* e, int32_t id, int64_t* steps, dou
   HostTissue* t = find_tissue(e, id);
   CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
   Engine& E = e->e;
-  cdb_status st = E.ensure_times(t->steps + 1);
+  cdb_status st = E.ensure_times(0);
   if (st != CDB_OK) return st;
   if (steps) *steps = t->steps;
-  if (time) *time = E.times[t->steps];
+  if (time) *time = E.tissue_time(*t);
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_set_clock(cdb_engine* e, int32_t id, int64_t loop, double time)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  CDB_CHECK(loop >= 0, CDB_INVALID_ARG, "loop must be >= 0");
+  Engine& E = e->e;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  t->steps = loop;
+  // clock 0 if its accumulated time at this step is exactly `time`
+  t->clock = 0;
+  cdb_status st = E.ensure_times(0);
+  if (st != CDB_OK) return st;
+  if (E.tissue_time(*t) != time) {
+    int c = -1;
+    for (size_t k = 1; k < E.clocks.size(); ++k)
+      if (E.clocks[k].base == loop && E.clocks[k].times[0] == time) c = (int)k;
+    if (c < 0) {
+      E.clocks.push_back(Engine::Clock{loop, {time}, 0});
+      c = (int)E.clocks.size() - 1;
+    }
+    t->clock = c;
+    st = E.ensure_times(0);
+    if (st != CDB_OK) return st;
+  }
+  E.dirty = true;
   return CDB_OK;
 }
 

@@ -51,6 +51,7 @@ struct TissueDev {
   int parity;             // buffer holding Vm at the start of the next launch batch
   int actAll;             // Vm was written by the host since the last step
   int64_t step0;          // steps taken at the start of the next launch batch
+  int64_t timeOff;        // time at step s is StepArgs::times[timeOff + s]
   double scale;           // diffusionScale (0: no diffusion)
   BlockScale blk;
   unsigned long long* minmax;   // 2 slots
@@ -223,8 +224,8 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, int t, int lane, co
   const WarpTile tile = a.tiles[t];
   const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
   const int64_t lstep = Tp->step0 + a.k;
-  const double time = a.times[lstep];
-  const double tnext = a.times[lstep + 1];
+  const double time = a.times[Tp->timeOff + lstep];
+  const double tnext = a.times[Tp->timeOff + lstep + 1];
   const bool active = lane < tile.count;
   // lanes past the tile's end stand in for its first cell until the end
   const int l = active ? lane : 0;

@@ -150,6 +150,10 @@ class Engine:
         _lib.check(_lib.load().cdb_engine_tissue_time(self.h, tid, ctypes.byref(s), ctypes.byref(t)))
         return s.value, t.value
 
+    def set_clock(self, tid, loop, time):
+        """A restart: the tissue continues from step `loop` at `time` (ms)."""
+        _lib.check(_lib.load().cdb_engine_set_clock(self.h, tid, int(loop), float(time)))
+
     def read_vm(self, tid):
         out = np.empty(self.tissues[tid])
         _lib.check(_lib.load().cdb_engine_read_vm(self.h, tid, _lib.dptr(out)))

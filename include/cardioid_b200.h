@@ -200,6 +200,11 @@ cdb_status cdb_engine_sync(cdb_engine* e);
 /* Number of steps a tissue has taken and its time (ms, accumulated as
  * time += dt like the reference). */
 cdb_status cdb_engine_tissue_time(cdb_engine* e, int32_t id, int64_t* steps, double* time);
+/* Sets a tissue's step count and time, as a restart does (the SIMULATE
+ * object's loop and time, written by writeRestart, elec/checkpointIO.cc:
+ * 104-117, and the checkpoint header): later steps continue time += dt from
+ * `time`.  Vm and state are unchanged (cdb_engine_write_vm/_write_state). */
+cdb_status cdb_engine_set_clock(cdb_engine* e, int32_t id, int64_t loop, double time);
 /* Host copies, cell order of the tissue. */
 cdb_status cdb_engine_read_vm(cdb_engine* e, int32_t id, double* host);
 cdb_status cdb_engine_write_vm(cdb_engine* e, int32_t id, const double* host);

@@ -35,6 +35,9 @@
 #include "object_cc.hh"
 #include "units.h"
 #include "PerformanceTimers.hh"
+#include "BucketOfBits.hh"
+#include "readPioFile.hh"
+#include "pio.h"
 
 Stimulus* stimulusFactory(const std::string& name, const Anatomy& anatomy);
 
@@ -283,6 +286,47 @@ void ref_sim_step(void* h, int nSteps)
          }
       }
    }
+}
+
+// Reads a pio file (name ends in '#', e.g. snapshot.000000000010/state#)
+// through the reference's own reader (simUtil/src/pio.c,
+// elec/readPioFile.cc, elec/BucketOfBits.cc), as readCheckpoint does
+// (elec/checkpointIO.cc:213-268).  Returns the record count (-1 if the file
+// cannot be opened); field names go space-separated into names; with values
+// given (capacity >= records x fields) every field of every record as a
+// double, record-major (u8 and int fields converted).
+long ref_read_pio(const char* name, int* nFields, char* names, int namesLen, double* values, long capacity)
+{
+   std::string first = std::string(name) + "000000";
+   if (access(first.c_str(), R_OK) != 0) return -1;
+   PFILE* file = Popen(name, "r", MPI_COMM_WORLD);
+   if (!file) return -1;
+   BucketOfBits* data = readPioFile(file);
+   Pclose(file);
+   const long n = data->nRecords();
+   const int nf = data->nFields();
+   *nFields = nf;
+   std::string all;
+   for (int f = 0; f < nf; ++f) all += (f ? " " : "") + data->fieldName(f);
+   if (names && namesLen > 0) {
+      std::strncpy(names, all.c_str(), namesLen - 1);
+      names[namesLen - 1] = 0;
+   }
+   if (values && capacity >= n * nf)
+      for (long r = 0; r < n; ++r) {
+         BucketOfBits::Record rec = data->getRecord(r);
+         for (int f = 0; f < nf; ++f) {
+            double v = 0;
+            switch (data->dataType(f)) {
+              case BucketOfBits::intType: { int t; rec.getValue(f, t); v = t; break; }
+              case BucketOfBits::u8Type: { uint64_t t; rec.getValue(f, t); v = (double)t; break; }
+              default: rec.getValue(f, v);
+            }
+            values[r * nf + f] = v;
+         }
+      }
+   delete data;
+   return n;
 }
 
 }  // extern "C"

@@ -49,6 +49,9 @@ def lib():
         L.ref_sim_set_state.argtypes = [vp, ctypes.c_char_p, dp]
         L.ref_sim_step.argtypes = [vp, ctypes.c_int]
         L.ref_set_threads.argtypes = [ctypes.c_int]
+        L.ref_read_pio.restype = ctypes.c_long
+        L.ref_read_pio.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_int, dp,
+                                   ctypes.c_long]
         _lib = L
     return _lib
 
@@ -158,3 +161,17 @@ class RefSim:
 
 def set_threads(n):
     lib().ref_set_threads(int(n))
+
+
+def read_pio(name):
+    """A pio file read by the reference's own reader: (field names, records x
+    fields array of doubles).  name ends in '#' (the files are name000000 ...)."""
+    L = lib()
+    nf = ctypes.c_int()
+    buf = ctypes.create_string_buffer(1 << 16)
+    n = L.ref_read_pio(name.encode(), ctypes.byref(nf), buf, len(buf), None, 0)
+    if n < 0:
+        raise FileNotFoundError(name)
+    out = np.empty((n, nf.value))
+    L.ref_read_pio(name.encode(), ctypes.byref(nf), buf, len(buf), _dp(out), out.size)
+    return buf.value.decode().split(), out
