@@ -62,7 +62,7 @@ struct TissueDev {
 // works on slot first + l, whose voxel in the padded Vm block is vox0 plus
 // the slot's offset (TissueDev::vrel).  Bit k of stimMask is set when
 // stimulus k's box holds a cell of the tile.
-struct WarpTile {
+struct __align__(16) WarpTile {
   int tissue;
   int count;
   int64_t first;
@@ -70,6 +70,7 @@ struct WarpTile {
   unsigned stimMask;
   int pad;
 };
+static_assert(sizeof(WarpTile) == 32, "tile descriptors are copied as two 16-byte chunks");
 
 struct StepArgs {
   TissueDev* tissues;
@@ -105,7 +106,7 @@ __host__ __device__ constexpr int vrel_offset()
 template <bool MIXED>
 __host__ __device__ constexpr int stage_bytes()
 {
-  return vrel_offset<MIXED>() + kBlk * 4;
+  return vrel_offset<MIXED>() + kBlk * 4 + 32;   // + the next tile's descriptor
 }
 
 __device__ __forceinline__ double pulse_value(const cdb_stimulus& s, double time)
@@ -193,11 +194,16 @@ __device__ __forceinline__ void warp_copy(unsigned char* dst, const unsigned cha
   for (int c = lane * 16; c < bytes; c += 32 * 16) cp_async16(dst + c, src + c);
 }
 
-// Copies tile t's state block (and, mixed, weight block) into buf.
-template <bool MIXED>
-__device__ __forceinline__ void stage_tile(const StepArgs& a, int t, int lane, unsigned char* buf)
+// Copies a 32-byte tile descriptor into shared memory (lanes 0 and 1).
+__device__ __forceinline__ void stage_desc(const WarpTile* src, WarpTile* dst, int lane)
 {
-  const WarpTile tile = a.tiles[t];
+  if (lane < 2) cp_async16((unsigned char*)dst + lane * 16, (const unsigned char*)src + lane * 16);
+}
+
+// Copies a tile's state block (and, mixed, weight block) into buf.
+template <bool MIXED>
+__device__ __forceinline__ void stage_tile(const StepArgs& a, const WarpTile& tile, int lane, unsigned char* buf)
+{
   const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
   const int64_t b = tile.first / kBlk;
   if (MIXED) {
@@ -218,10 +224,10 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, int t, int lane, u
 // One tile.  With `staged` the tile's state (and mixed weights) are read
 // from buf; otherwise straight from global memory.
 template <bool MIXED, int SLOT>
-__device__ __forceinline__ void step_tile(const StepArgs& a, int t, int lane, const unsigned char* buf, bool staged)
+__device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& tile, int lane, const unsigned char* buf,
+                                          bool staged)
 {
   constexpr bool SPEC = SLOT >= 0;
-  const WarpTile tile = a.tiles[t];
   const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
   const int64_t lstep = Tp->step0 + a.k;
   const double time = a.times[Tp->timeOff + lstep];
@@ -338,14 +344,14 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, int t, int lane, co
   }
 }
 
-// Resident CTAs per SM the register budget aims at: at least 4 CTAs (16
-// warps, at most 128 registers).  Both steps fit there without spilling; the
-// mixed one uses few enough registers for 5 (shared memory then caps it).
+// Resident CTAs per SM the register budget aims at: 4 for FP64 (16 warps,
+// at most 128 registers) and 5 for mixed (20 warps, at most 102 registers,
+// which its shared-memory buffers also allow); neither spills.
 #ifndef CDB_FP64_MIN_CTAS
 #define CDB_FP64_MIN_CTAS 4
 #endif
 template <bool MIXED>
-constexpr int min_ctas() { return MIXED ? 4 : CDB_FP64_MIN_CTAS; }
+constexpr int min_ctas() { return MIXED ? 5 : CDB_FP64_MIN_CTAS; }
 
 // Persistent over the launch's warp tiles: warp w takes tiles w, w + W,
 // w + 2W, ... (W warps in the grid).  With a.stage set, the next tile's
@@ -365,19 +371,41 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
   const int stride = gridDim.x * kWarpsPerCta;
   int t = blockIdx.x * kWarpsPerCta + warpInCta;
   if (!a.stage) {
-    for (; t < a.nTiles; t += stride) step_tile<MIXED, SLOT>(a, t, lane, nullptr, false);
+    // the next tile's descriptor is in flight while this tile computes
+    WarpTile cur, nxt;
+    if (t < a.nTiles) cur = a.tiles[t];
+    for (; t < a.nTiles; t += stride) {
+      if (t + stride < a.nTiles) nxt = a.tiles[t + stride];
+      step_tile<MIXED, SLOT>(a, cur, lane, nullptr, false);
+      cur = nxt;
+    }
     return;
   }
-  if (t < a.nTiles) stage_tile<MIXED>(a, t, lane, mine);
+  // Buffer i holds tile t's inputs and the descriptor of tile t + stride,
+  // copied together one iteration ahead.
+  WarpTile* desc0 = (WarpTile*)(mine + vrel_offset<MIXED>() + kBlk * 4);
+  WarpTile* desc1 = (WarpTile*)(mine + kBuf + vrel_offset<MIXED>() + kBlk * 4);
+  if (t < a.nTiles) {
+    const WarpTile first = a.tiles[t];
+    stage_tile<MIXED>(a, first, lane, mine);
+    if (t + stride < a.nTiles) stage_desc(a.tiles + t + stride, desc0, lane);
+  }
   cp_async_commit();
+  WarpTile cur = t < a.nTiles ? a.tiles[t] : WarpTile{};
   for (int it = 0; t < a.nTiles; ++it, t += stride) {
     const int tn = t + stride;
-    __syncwarp();   // every lane is done with the buffer refilled next
-    if (tn < a.nTiles) stage_tile<MIXED>(a, tn, lane, mine + ((it + 1) & 1) * kBuf);
+    WarpTile* mineDesc = (it & 1) ? desc1 : desc0;        // descriptor of tile tn, copied with tile t
+    WarpTile* nextDesc = (it & 1) ? desc0 : desc1;
+    cp_async_wait_all();    // tile t's inputs and tile tn's descriptor (copied during the last tile) have landed
+    __syncwarp();           // for every lane, and every lane is done with the other buffer
+    const WarpTile nxt = tn < a.nTiles ? *mineDesc : WarpTile{};
+    if (tn < a.nTiles) {
+      stage_tile<MIXED>(a, nxt, lane, mine + ((it + 1) & 1) * kBuf);
+      if (tn + stride < a.nTiles) stage_desc(a.tiles + tn + stride, nextDesc, lane);
+    }
     cp_async_commit();
-    cp_async_wait_prev();   // this thread's copies of tile t have landed
-    __syncwarp();           // and so have the other lanes'
-    step_tile<MIXED, SLOT>(a, t, lane, mine + (it & 1) * kBuf, true);
+    step_tile<MIXED, SLOT>(a, cur, lane, mine + (it & 1) * kBuf, true);
+    cur = nxt;
   }
   cp_async_wait_all();
 }

@@ -65,23 +65,31 @@ struct BlockScale {
 };
 
 // FP64 quotient without the slow-path branch of the IEEE division: the
-// hardware reciprocal approximation (PTX rcp.approx.ftz.f64) refined by two
-// Newton-Raphson steps r <- r + r (1 - b r), then the quotient corrected
+// hardware reciprocal approximation (PTX rcp.approx.ftz.f64) refined by one
+// Newton-Raphson step r <- r + r (1 - b r), then the quotient corrected
 // once by its residual, q <- q + r (a - b q) (Markstein's method, IBM J.
-// Res. Dev. 34(1), 1990).  Within a few ulp of a / b for the normal,
+// Res. Dev. 34(1), 1990): the correction squares the reciprocal's relative
+// error, so one refinement of the seed is enough for a faithful quotient.  Within a few ulp of a / b for the normal,
 // finite operands of the model (tests/test_division_gpu.py measures it
 // against CUDA's a / b); subnormal divisors flush to zero.  Defining
 // CDB_IEEE_DIV restores a / b.
+// The seed refined once (relative error about the square of the seed's).
+__device__ __forceinline__ double rcp64_1(double b)
+{
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+  const double e = fma(-b, r, 1.0);
+  return fma(r, e, r);
+}
+
+// A reciprocal on its own: refined twice.
 __device__ __forceinline__ double rcp64(double b)
 {
 #ifdef CDB_IEEE_DIV
   return 1.0 / b;
 #else
-  double r;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
-  double e = fma(-b, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-b, r, 1.0);
+  const double r = rcp64_1(b);
+  const double e = fma(-b, r, 1.0);
   return fma(r, e, r);
 #endif
 }
@@ -91,7 +99,7 @@ __device__ __forceinline__ double div64(double a, double b)
 #ifdef CDB_IEEE_DIV
   return a / b;
 #else
-  const double r = rcp64(b);
+  const double r = rcp64_1(b);
   const double q = a * r;
   return fma(r, fma(-b, q, a), q);
 #endif

@@ -1,5 +1,5 @@
 """The engine's branch-free FP64 quotient (div64: hardware reciprocal seed,
-two Newton-Raphson steps, one residual correction) against CUDA's IEEE
+one Newton-Raphson step, one residual correction) against CUDA's IEEE
 a / b on operands spanning the model's range: at most 2 ulp away."""
 import ctypes
 
