@@ -143,6 +143,8 @@ inline TT06Scalars to_scalars(const cdb_tt06_params& p)
   TT06Scalars s;
   s.celltype = p.celltype; s.g_CaL = p.g_CaL; s.g_K1 = p.g_K1; s.g_Kr = p.g_Kr; s.g_Ks = p.g_Ks;
   s.g_Na = p.g_Na; s.g_bca = p.g_bca; s.g_bna = p.g_bna; s.g_pCa = p.g_pCa; s.g_pK = p.g_pK; s.g_to = p.g_to;
+  s.f_Ks = (float)p.g_Ks; s.f_bca = (float)p.g_bca; s.f_bna = (float)p.g_bna; s.f_pCa = (float)p.g_pCa;
+  s.f_pK = (float)p.g_pK; s.f_to = (float)p.g_to;
   return s;
 }
 

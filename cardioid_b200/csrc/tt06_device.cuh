@@ -46,7 +46,18 @@ enum StateSlot {
 // Scalar parameters of one reaction type (REACTION object).
 struct TT06Scalars {
   double celltype, g_CaL, g_K1, g_Kr, g_Ks, g_Na, g_bca, g_bna, g_pCa, g_pK, g_to;
+  // FP32 copies for the mixed step (constant operands, no conversion)
+  float f_Ks, f_bca, f_bna, f_pCa, f_pK, f_to;
 };
+
+// FP32 quotient from the hardware reciprocal approximation
+// (rcp.approx.ftz.f32, within 1 ulp): a * (1/b), no range handling.
+__device__ __forceinline__ float fdiv(float a, float b)
+{
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+  return a * r;
+}
 
 // Shape of the 30 fits of one reaction type: term counts and the offset of
 // each fit's coefficients inside the type's coefficient pool.
@@ -133,7 +144,7 @@ __device__ __forceinline__ float fit_eval_fast(const float* __restrict__ c, int 
 #pragma unroll 2
   for (int k = denom - 3; k >= 0; --k) den = fmaf(x, den, d[k]);
   den = fmaf(x, den, 1.0f);
-  return __fdividef(num, den);
+  return fdiv(num, den);
 }
 
 // The same with compile-time term counts and offsets (fully unrolled).
@@ -164,7 +175,7 @@ __device__ __forceinline__ float fit_spec32(const float* __restrict__ c, float x
 #pragma unroll
   for (int k = D - 3; k >= 0; --k) den = fmaf(x, den, c[O + N + k]);
   den = fmaf(x, den, 1.0f);
-  return __fdividef(num, den);
+  return fdiv(num, den);
 }
 
 // FP32 fits of V in the power basis: with pw[k] = V^k computed once per
@@ -187,7 +198,7 @@ __device__ __forceinline__ float fit_pow32(const float* __restrict__ c, const fl
   float den = fmaf(pw[1], c[O + N], 1.0f);
 #pragma unroll
   for (int k = 2; k < D; ++k) den = fmaf(pw[k], c[O + N + k - 1], den);
-  return __fdividef(num, den);
+  return fdiv(num, den);
 }
 
 // The largest power any FP32-evaluated V-fit of the compiled shapes needs.

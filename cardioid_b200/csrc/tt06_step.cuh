@@ -151,42 +151,42 @@ __device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const Blo
   const float calT3 = FIT(F_CalT3, Vf), calT4 = FIT(F_CalT4, Vf);
   // __logf (hardware log2, ~2^-21 relative): the Nernst potentials need
   // ~1e-6 mV, and their arguments are positive concentration ratios
-  const float eCa = 0.5f * RT_F * __logf(__fdividef(Cao, caI));
-  const float iBCa = (float)p.g_bca * (Vf - eCa);
-  const float iPCa = __fdividef(caI * (float)p.g_pCa, caI + KpCa);
+  const float eCa = 0.5f * RT_F * __logf(fdiv(Cao, caI));
+  const float iBCa = p.f_bca * (Vf - eCa);
+  const float iPCa = fdiv(caI * p.f_pCa, caI + KpCa);
   const float expG = FIT(F_expG, Vf), expGm1 = FIT(F_expGm1, Vf);
   const float pKterm = FIT(F_pKterm, Vf);
-  const float eK = RT_F * __logf(__fdividef(Ko, kI));
+  const float eK = RT_F * __logf(fdiv(Ko, kI));
   const float naKterm = FIT(F_NaKterm, Vf);
-  const float iNaK = __fdividef(naI * naKterm, naI + KmNa);
+  const float iNaK = fdiv(naI * naKterm, naI + KmNa);
   const float vEK = Vf - eK;
   const float cC = caI + KbufC, cSR = caSR + KbufSr, cSS = caSS + KbufSs;
-  const float bufC = __fdividef(1.0f, __fdividef(BufC * KbufC, cC * cC) + 1.0f);
-  const float bufSR = __fdividef(1.0f, __fdividef(BufSr * KbufSr, cSR * cSR) + 1.0f);
-  const float bufSS = __fdividef(1.0f, __fdividef(BufSs * KbufSs, cSS * cSS) + 1.0f);
+  const float bufC = fdiv(1.0f, fdiv(BufC * KbufC, cC * cC) + 1.0f);
+  const float bufSR = fdiv(1.0f, fdiv(BufSr * KbufSr, cSR * cSR) + 1.0f);
+  const float bufSS = fdiv(1.0f, fdiv(BufSs * KbufSs, cSS * cSS) + 1.0f);
   const float iLeak = Vleak * (caSR - caI);
-  const float iUp = __fdividef(VmaxUp, 1.0f + __fdividef(Kup2, caI * caI));
+  const float iUp = fdiv(VmaxUp, 1.0f + fdiv(Kup2, caI * caI));
   const float iXfer = Vxfer * (caSS - caI);
-  const float kcasr = MaxSr - __fdividef(MaxSr - MinSr, 1.0f + __fdividef(EC2, caSR * caSR));
-  const float k1 = __fdividef(K1p, kcasr), k2 = K2p * kcasr;
+  const float kcasr = MaxSr - fdiv(MaxSr - MinSr, 1.0f + fdiv(EC2, caSR * caSR));
+  const float k1 = fdiv(K1p, kcasr), k2 = K2p * kcasr;
   const float ss2 = caSS * caSS;
-  const float O = __fdividef(ss2 * rPrime * k1, ss2 * k1 + K3);
+  const float O = fdiv(ss2 * rPrime * k1, ss2 * k1 + K3);
   const float dRprime = -caSS * rPrime * k2 + K4 * (1.0f - rPrime);
   const float iRel = O * Vrel * (caSR - caSS);
   const float dCaSR = bufSR * (iUp - iLeak - iRel);
   const float iCaL = d * f * f2 * fCass * gCaL * (0.25f * caSS * calT4 - Cao * calT3);
   constexpr float nao3 = Nao * Nao * Nao, kmnai3 = KmNai * KmNai * KmNai;
   constexpr float naCaDen0 = (nao3 + kmnai3) * (Cao + KmCa);
-  const float iNaCa = __fdividef(KNaCa * ((naI * naI * naI) * Cao * expG - nao3 * caI * Alpha * expGm1),
+  const float iNaCa = fdiv(KNaCa * ((naI * naI * naI) * Cao * expG - nao3 * caI * Alpha * expGm1),
                                  naCaDen0 * (Ksat * expGm1 + 1.0f));
   const float iK1 = FITX(F_K1, vEK, V - (double)eK);
-  const float iPK = vEK * (float)p.g_pK * pKterm;
+  const float iPK = vEK * p.f_pK * pKterm;
   const float iKr = 0.430331482911935f * 2.3237900077f * vEK * Xr1 * Xr2 * gKr;
-  const float eNa = RT_F * __logf(__fdividef(Nao, naI));
-  const float eKs = RT_F * __logf(__fdividef(Ko + Nao * Pkna, kI + naI * Pkna));
-  const float iKs = (Xs * Xs) * (float)p.g_Ks * (Vf - eKs);
-  const float iBNa = (float)p.g_bna * (Vf - eNa);
-  const float iTo = vEK * (float)p.g_to * r * s;
+  const float eNa = RT_F * __logf(fdiv(Nao, naI));
+  const float eKs = RT_F * __logf(fdiv(Ko + Nao * Pkna, kI + naI * Pkna));
+  const float iKs = (Xs * Xs) * p.f_Ks * (Vf - eKs);
+  const float iBNa = p.f_bna * (Vf - eNa);
+  const float iTo = vEK * p.f_to * r * s;
   const float kTot = -2.0f * iNaK + iK1 + iPK + iKr + iKs + iTo;
   constexpr float halfCm_FVc = -0.5f * Cm / (F * Vc), halfCm_FVss = -0.5f * Cm / (F * Vss);
   const float dCaI = bufC * (halfCm_FVc * (iBCa + iPCa - 2.0f * iNaCa) + iXfer + (Vsr / Vc) * (iLeak - iUp));
@@ -219,7 +219,7 @@ __device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const Blo
   GATE(S_f, f, F_f_a, F_f_b)
   GATE(S_f2, f2, F_f2_a, F_f2_b)
   {
-    const float fCassInf = 0.4f + __fdividef(0.6f, 400.0f * (caSS * caSS) + 1.0f);
+    const float fCassInf = 0.4f + fdiv(0.6f, 400.0f * (caSS * caSS) + 1.0f);
     const float ga = FITX(F_fCass_a, caSS, caSSd), gb = -fCassInf;
     io.template put<S_fCass>(fCass + ga * (fCass + gb));
   }
