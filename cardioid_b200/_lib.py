@@ -115,6 +115,8 @@ def load():
         "cdb_engine_sync": (st, [vp]),
         "cdb_engine_tissue_time": (st, [vp, ctypes.c_int32, i64p, dp]),
         "cdb_engine_set_clock": (st, [vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_double]),
+        "cdb_engine_set_ecg": (st, [vp, ctypes.c_int32, ctypes.c_int32, dp, ctypes.c_int32, ctypes.c_double]),
+        "cdb_engine_read_ecg": (st, [vp, ctypes.c_int32, ctypes.c_int64, i64p, i64p, dp]),
         "cdb_engine_read_vm": (st, [vp, ctypes.c_int32, dp]),
         "cdb_engine_write_vm": (st, [vp, ctypes.c_int32, dp]),
         "cdb_engine_read_state": (st, [vp, ctypes.c_int32, ctypes.c_int, dp]),

@@ -74,6 +74,9 @@ struct HostTissue {
   int64_t nSlots = 0;               // AoSoA slots (cells plus padding)
   std::vector<int64_t> slot;        // slot of every cell
   DeviceBuffer slotMap, vrel;       // device copies: cell -> slot; per-slot voxel offsets
+  DeviceBuffer ecgPts, ecgTrace;    // ECG electrodes and trace ring (cdb_engine_set_ecg)
+  double ecgK = 0;                  // kconst * dx dy dz
+  int64_t ecgNext = 0;              // next evaluation (step / rate) to hand to the host
   int64_t steps = 0;       // steps taken
   int clock = 0;           // its time sequence (Engine::clocks)
   int parity = 0;
@@ -701,6 +704,7 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
   d.act = h->act.as<double>();
   d.minmax = h->minmax.as<unsigned long long>();
   d.actAll = 1;
+  d.hx = t->dx; d.hy = t->dy; d.hz = t->dz;
   d.vrel = h->vrel.as<int>();
   init_state_kernel<<<grid_for(nSlots, 256), 256, 0, s>>>(nSlots, d.s64, d.s32, mixed ? 1 : 0, d.act);
   E.launches += 1;
@@ -764,6 +768,67 @@ cdb_status cdb_engine_tissue_time(cdb_engine* e, int32_t id, int64_t* steps, dou
   if (st != CDB_OK) return st;
   if (steps) *steps = t->steps;
   if (time) *time = E.tissue_time(*t);
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_set_ecg(cdb_engine* e, int32_t id, int32_t nPoints, const double* xyz, int32_t evalRate,
+                              double kconst)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  CDB_CHECK(nPoints >= 0 && nPoints <= kEcgMaxPoints, CDB_INVALID_ARG, "ECG needs 0..32 electrodes");
+  CDB_CHECK(nPoints == 0 || (xyz && evalRate >= 1), CDB_INVALID_ARG, "ECG electrodes and an evalRate >= 1 are required");
+  Engine& E = e->e;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  TissueDev& d = t->dev;
+  if (nPoints == 0) {
+    d.ecgN = 0;
+    t->ecgPts.release();
+    t->ecgTrace.release();
+  } else {
+    CDB_CUDA(t->ecgPts.alloc(nPoints * 3 * sizeof(double)));
+    CDB_CUDA(cudaMemcpy(t->ecgPts.p, xyz, nPoints * 3 * sizeof(double), cudaMemcpyHostToDevice));
+    CDB_CUDA(t->ecgTrace.alloc((size_t)kEcgRing * nPoints * sizeof(double)));
+    CDB_CUDA(cudaMemset(t->ecgTrace.p, 0, (size_t)kEcgRing * nPoints * sizeof(double)));
+    d.ecgN = nPoints;
+    d.ecgRate = evalRate;
+    t->ecgK = kconst * d.hx * d.hy * d.hz;
+    t->ecgNext = t->steps / evalRate + 1;
+  }
+  d.ecgPts = t->ecgPts.as<double>();
+  d.ecgTrace = t->ecgTrace.as<double>();
+  E.dirty = true;
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_read_ecg(cdb_engine* e, int32_t id, int64_t maxEntries, int64_t* nEntries, int64_t* loops,
+                               double* values)
+{
+  CDB_CHECK(e && nEntries, CDB_INVALID_ARG, "null argument");
+  HostTissue* t = find_tissue(e, id);
+  CDB_CHECK(t, CDB_NOT_FOUND, "no tissue with that id");
+  *nEntries = 0;
+  const TissueDev& d = t->dev;
+  if (d.ecgN == 0) return CDB_OK;
+  CDB_CHECK(maxEntries >= 0 && (maxEntries == 0 || (loops && values)), CDB_INVALID_ARG, "output arrays are required");
+  Engine& E = e->e;
+  CDB_CUDA(cudaSetDevice(E.cfg.device));
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  const int64_t last = t->steps / d.ecgRate;                  // last completed evaluation
+  // the ring holds the last kEcgRing - 1 evaluations (each one clears the next entry)
+  const int64_t first = std::max(t->ecgNext, last - kEcgRing + 2);
+  const int64_t n = std::min<int64_t>(std::max<int64_t>(0, last - first + 1), maxEntries);
+  std::vector<double> ring((size_t)kEcgRing * d.ecgN);
+  if (n > 0) CDB_CUDA(cudaMemcpy(ring.data(), t->ecgTrace.p, ring.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int64_t k = 0; k < n; ++k) {
+    const int64_t ev = first + k;
+    loops[k] = ev * d.ecgRate;
+    for (int j = 0; j < d.ecgN; ++j) values[k * d.ecgN + j] = ring[(size_t)(ev % kEcgRing) * d.ecgN + j] * t->ecgK;
+  }
+  t->ecgNext = first + n;
+  *nEntries = n;
   return CDB_OK;
 }
 

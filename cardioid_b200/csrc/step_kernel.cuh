@@ -55,6 +55,13 @@ struct TissueDev {
   double scale;           // diffusionScale (0: no diffusion)
   BlockScale blk;
   unsigned long long* minmax;   // 2 slots
+  // ECG pseudo-sensor (off when ecgN == 0): electrodes at ecgPts (x y z, mm),
+  // evaluated when the step count reaches a multiple of ecgRate into entry
+  // (count / ecgRate) % kEcgRing of ecgTrace ([kEcgRing][ecgN]).
+  int ecgN, ecgRate;
+  const double* ecgPts;
+  double* ecgTrace;
+  double hx, hy, hz;          // voxel spacing, mm
 };
 
 // A warp tile: one 32-slot AoSoA block of one tissue, whose slots hold
@@ -71,6 +78,17 @@ struct __align__(16) WarpTile {
   int pad;
 };
 static_assert(sizeof(WarpTile) == 32, "tile descriptors are copied as two 16-byte chunks");
+
+constexpr int kEcgRing = 1024;
+constexpr int kEcgMaxPoints = 32;
+
+// A warp's running ECG sum (lane j: electrode j) for one tissue and one
+// evaluation entry, added to the trace when either changes.
+struct EcgAcc {
+  double v;
+  int tissue;
+  int entry;
+};
 
 struct StepArgs {
   TissueDev* tissues;
@@ -221,11 +239,21 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, const WarpTile& ti
   warp_copy(buf + vrel_offset<MIXED>(), (const unsigned char*)(Tp->vrel + b * kBlk), kBlk * 4, lane);
 }
 
+__device__ __forceinline__ void ecg_flush(const StepArgs& a, EcgAcc& acc, int lane)
+{
+  if (acc.tissue >= 0) {
+    const TissueDev* __restrict__ T = a.tissues + acc.tissue;
+    if (lane < T->ecgN) atomicAdd(T->ecgTrace + (int64_t)acc.entry * T->ecgN + lane, acc.v);
+  }
+  acc.tissue = -1;
+  acc.v = 0.0;
+}
+
 // One tile.  With `staged` the tile's state (and mixed weights) are read
 // from buf; otherwise straight from global memory.
 template <bool MIXED, int SLOT>
 __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& tile, int lane, const unsigned char* buf,
-                                          bool staged)
+                                          bool staged, EcgAcc& ecg)
 {
   constexpr bool SPEC = SLOT >= 0;
   const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
@@ -258,6 +286,7 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
     }
   }
   double vnew = 0.0;
+  double ecgSrc = 0.0;        // the cell's dVmD, the ECG's source term
   if (active) {
     const int cur = (Tp->parity + a.k) & 1;
     const double* __restrict__ vin = Tp->vm[cur];
@@ -288,6 +317,7 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
       }
       dvmD = acc * scale;
     }
+    ecgSrc = dvmD;
 
     // With SPEC the slot is a template parameter, so every coefficient
     // address is a compile-time constant.
@@ -342,6 +372,32 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
       atomicMax(Tp->minmax + 1, ordered_bits(hi));
     }
   }
+  // ECG (ECGSensor::eval / calcEcg, elec/ECGSensor.cc:231-320 and
+  // elec/ECGSensor.cu:9-168): after the step, on evaluation steps, electrode
+  // j gets sum over cells of dVmD / |r - p_j| with r = (x dx, y dy, z dz).
+  const int ecgN = Tp->ecgN;
+  if (ecgN && (lstep + 1) % Tp->ecgRate == 0) {
+    const int entry = (int)(((lstep + 1) / Tp->ecgRate) % kEcgRing);
+    if (ecg.tissue != tile.tissue || ecg.entry != entry) {
+      ecg_flush(a, ecg, lane);
+      ecg.tissue = tile.tissue;
+      ecg.entry = entry;
+    }
+    const int64_t zz = vox / pxy, rem = vox - zz * pxy, yy = rem / px;
+    const double xr = (double)((int)(rem - yy * px) - 1) * Tp->hx;
+    const double yr = (double)((int)yy - Tp->py0) * Tp->hy;
+    const double zr = (double)((int)zz - Tp->pz0) * Tp->hz;
+    for (int j = 0; j < ecgN; ++j) {
+      const double* p = Tp->ecgPts + 3 * j;
+      const double ex = xr - p[0], ey = yr - p[1], ez = zr - p[2];
+      double c = active ? ecgSrc * (1.0 / sqrt(ex * ex + ey * ey + ez * ez)) : 0.0;
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      if (lane == j) ecg.v += c;
+    }
+    // the tissue's first tile clears the entry the next evaluation fills
+    if (tile.first == 0 && lane < ecgN)
+      Tp->ecgTrace[(int64_t)((entry + 1) % kEcgRing) * ecgN + lane] = 0.0;
+  }
 }
 
 // Resident CTAs per SM the register budget aims at: 4 for FP64 (16 warps,
@@ -373,12 +429,14 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
   if (!a.stage) {
     // the next tile's descriptor is in flight while this tile computes
     WarpTile cur, nxt;
+    EcgAcc ecg{0.0, -1, 0};
     if (t < a.nTiles) cur = a.tiles[t];
     for (; t < a.nTiles; t += stride) {
       if (t + stride < a.nTiles) nxt = a.tiles[t + stride];
-      step_tile<MIXED, SLOT>(a, cur, lane, nullptr, false);
+      step_tile<MIXED, SLOT>(a, cur, lane, nullptr, false, ecg);
       cur = nxt;
     }
+    ecg_flush(a, ecg, lane);
     return;
   }
   // Buffer i holds tile t's inputs and the descriptor of tile t + stride,
@@ -392,6 +450,7 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
   }
   cp_async_commit();
   WarpTile cur = t < a.nTiles ? a.tiles[t] : WarpTile{};
+  EcgAcc ecg{0.0, -1, 0};
   for (int it = 0; t < a.nTiles; ++it, t += stride) {
     const int tn = t + stride;
     WarpTile* mineDesc = (it & 1) ? desc1 : desc0;        // descriptor of tile tn, copied with tile t
@@ -404,10 +463,11 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
       if (tn + stride < a.nTiles) stage_desc(a.tiles + tn + stride, nextDesc, lane);
     }
     cp_async_commit();
-    step_tile<MIXED, SLOT>(a, cur, lane, mine + (it & 1) * kBuf, true);
+    step_tile<MIXED, SLOT>(a, cur, lane, mine + (it & 1) * kBuf, true, ecg);
     cur = nxt;
   }
   cp_async_wait_all();
+  ecg_flush(a, ecg, lane);
 }
 
 // The compiled kernel of a slot when the type has the compiled fit shapes

@@ -154,6 +154,26 @@ class Engine:
         """A restart: the tissue continues from step `loop` at `time` (ms)."""
         _lib.check(_lib.load().cdb_engine_set_clock(self.h, tid, int(loop), float(time)))
 
+    def set_ecg(self, tid, points, eval_rate, kconst=1.0):
+        """Fused ECG pseudo-sensor: electrodes points (n x 3, mm), evaluated
+        every eval_rate steps (ECGSensor)."""
+        pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        self._ecg_n = {**getattr(self, "_ecg_n", {}), tid: len(pts)}
+        _lib.check(_lib.load().cdb_engine_set_ecg(self.h, tid, len(pts), _lib.dptr(pts), int(eval_rate),
+                                                  float(kconst)))
+
+    def read_ecg(self, tid, max_entries=1024):
+        """(loops, values[entries, electrodes]) of the evaluations not read yet."""
+        n = self._ecg_n.get(tid, 0)
+        loops = np.empty(max_entries, np.int64)
+        vals = np.empty(max_entries * max(n, 1))
+        cnt = ctypes.c_int64()
+        _lib.check(_lib.load().cdb_engine_read_ecg(
+            self.h, tid, max_entries, ctypes.byref(cnt), loops.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+            _lib.dptr(vals)))
+        k = cnt.value
+        return loops[:k].copy(), vals[:k * n].reshape(k, n)
+
     def read_vm(self, tid):
         out = np.empty(self.tissues[tid])
         _lib.check(_lib.load().cdb_engine_read_vm(self.h, tid, _lib.dptr(out)))

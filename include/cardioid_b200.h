@@ -205,6 +205,18 @@ cdb_status cdb_engine_tissue_time(cdb_engine* e, int32_t id, int64_t* steps, dou
  * 104-117, and the checkpoint header): later steps continue time += dt from
  * `time`.  Vm and state are unchanged (cdb_engine_write_vm/_write_state). */
 cdb_status cdb_engine_set_clock(cdb_engine* e, int32_t id, int64_t loop, double time);
+/* The ECG pseudo-sensor fused into the step (ECGSensor, elec/ECGSensor.cc:
+ * 20-320, elec/ECGSensor.cu:9-168): every evalRate steps, electrode j
+ * (xyz[3j..3j+2], mm) records kconst dx dy dz sum over cells of
+ * dVmD / |r - p_j|, r = (x dx, y dy, z dz) from the cell's gid.  At most 32
+ * electrodes; nPoints = 0 turns it off.  The device keeps the last 1023
+ * evaluations; cdb_engine_read_ecg hands out those not read yet (oldest
+ * first): loops[k] is the step count of evaluation k and values[k*nPoints+j]
+ * its electrode j. */
+cdb_status cdb_engine_set_ecg(cdb_engine* e, int32_t id, int32_t nPoints, const double* xyz, int32_t evalRate,
+                              double kconst);
+cdb_status cdb_engine_read_ecg(cdb_engine* e, int32_t id, int64_t maxEntries, int64_t* nEntries, int64_t* loops,
+                               double* values);
 /* Host copies, cell order of the tissue. */
 cdb_status cdb_engine_read_vm(cdb_engine* e, int32_t id, double* host);
 cdb_status cdb_engine_write_vm(cdb_engine* e, int32_t id, const double* host);
