@@ -102,6 +102,13 @@ def load():
         "cdb_fgr_calc": (st, [vp, vp, vp]),
         "cdb_fgr_get_weights": (st, [vp, dp]),
         "cdb_fgr_destroy": (st, [vp]),
+        "cdb_diff6_create": (st, [ctypes.c_int, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                  ctypes.c_double, ctypes.c_double, ctypes.c_int64, i64p, dp, ctypes.c_double,
+                                  ctypes.POINTER(ctypes.c_void_p)]),
+        "cdb_diff6_update_local_voltage": (st, [vp, vp, vp]),
+        "cdb_diff6_calc": (st, [vp, vp, vp]),
+        "cdb_diff6_get_face_sigma": (st, [vp, dp]),
+        "cdb_diff6_destroy": (st, [vp]),
         "cdb_fgr_calc_static": (st, [ctypes.c_int, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp, vp, vp,
                                      ctypes.c_double, vp]),
         "cdb_engine_create": (st, [ctypes.POINTER(EngineConfig), vpp]),

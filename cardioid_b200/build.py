@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libcardioid_b200.so")
-SOURCES = ["engine_host.cu", "plugins.cu", "static_scratch.cu"]
+SOURCES = ["engine_host.cu", "plugins.cu", "static_scratch.cu", "diff6.cu"]
 HEADERS = ["common.cuh", "tt06_device.cuh", "tt06_step.cuh", "fgr_device.cuh", "step_kernel.cuh", "fit_shapes.h",
            os.path.join("..", "..", "include", "cardioid_b200.h")]
 

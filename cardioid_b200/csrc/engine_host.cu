@@ -144,13 +144,14 @@ struct Engine {
   int stage = 1;           // 1: stage each warp's next tile through shared memory (cp.async)
   int ctasPerSm = 0;       // persistent grid: SMs x this; 0 = as many as are resident
   int numSms = 148;
-  int resident[CDB_MAX_REACTION_TYPES + 1] = {};   // resident CTAs per SM by slot (last: generic)
+  int resident[2][CDB_MAX_REACTION_TYPES + 1] = {};   // resident CTAs per SM by [ECG][slot] (last: generic)
+  bool anyEcg = false;     // a tissue has ECG electrodes: launch the kernels with the sensor
 
   int grid_ctas_per_sm(int slot)
   {
     if (ctasPerSm > 0) return ctasPerSm;
-    int& r = resident[slot < 0 ? CDB_MAX_REACTION_TYPES : slot];
-    if (r == 0) r = cfg.precision == CDB_MIXED ? resident_ctas<true>(slot) : resident_ctas<false>(slot);
+    int& r = resident[anyEcg ? 1 : 0][slot < 0 ? CDB_MAX_REACTION_TYPES : slot];
+    if (r == 0) r = cfg.precision == CDB_MIXED ? resident_ctas<true>(slot, anyEcg) : resident_ctas<false>(slot, anyEcg);
     return r > 0 ? r : 4;
   }
 
@@ -209,8 +210,10 @@ struct Engine {
     std::vector<WarpTile> tiles;
     std::vector<WarpTile> bySlot[CDB_MAX_REACTION_TYPES];
     std::vector<cdb_stimulus> stims;
+    anyEcg = false;
     for (auto& kv : tissues) {
       HostTissue& t = *kv.second;
+      anyEcg = anyEcg || t.dev.ecgN > 0;
       t.dev.stim0 = (int)stims.size();
       t.dev.nstim = (int)t.stims.size();
       stims.insert(stims.end(), t.stims.begin(), t.stims.end());
@@ -290,8 +293,8 @@ struct Engine {
         const int slot = spec[st.first] ? st.first : -1;
         const unsigned grid = (unsigned)std::min<int64_t>(grid_for(a.nTiles, kWarpsPerCta),
                                                           (int64_t)numSms * grid_ctas_per_sm(slot));
-        if (cfg.precision == CDB_MIXED) launch_step<true>(slot, grid, stream, a);
-        else launch_step<false>(slot, grid, stream, a);
+        if (cfg.precision == CDB_MIXED) launch_step<true>(slot, anyEcg, grid, stream, a);
+        else launch_step<false>(slot, anyEcg, grid, stream, a);
         ++launches;
       }
     }

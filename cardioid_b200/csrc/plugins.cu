@@ -7,7 +7,7 @@
 //                   elec/FGRDiffusionOMP.cc:75-131): updateLocalVoltage scatters
 //                   Vm into the padded block, calc assigns dVm.
 // They keep the reference's data flow (Vm crosses HBM several times per
-// step); the fused engine (engine.cu) is the fast path.
+// step); the fused engine (engine_host.cu) is the fast path.
 #include <cuda_runtime.h>
 
 #include <memory>

@@ -251,7 +251,7 @@ __device__ __forceinline__ void ecg_flush(const StepArgs& a, EcgAcc& acc, int la
 
 // One tile.  With `staged` the tile's state (and mixed weights) are read
 // from buf; otherwise straight from global memory.
-template <bool MIXED, int SLOT>
+template <bool MIXED, int SLOT, bool ECG>
 __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& tile, int lane, const unsigned char* buf,
                                           bool staged, EcgAcc& ecg)
 {
@@ -375,8 +375,8 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
   // ECG (ECGSensor::eval / calcEcg, elec/ECGSensor.cc:231-320 and
   // elec/ECGSensor.cu:9-168): after the step, on evaluation steps, electrode
   // j gets sum over cells of dVmD / |r - p_j| with r = (x dx, y dy, z dz).
-  const int ecgN = Tp->ecgN;
-  if (ecgN && (lstep + 1) % Tp->ecgRate == 0) {
+  const int ecgN = ECG ? Tp->ecgN : 0;
+  if (ECG && ecgN && (lstep + 1) % Tp->ecgRate == 0) {
     const int entry = (int)(((lstep + 1) / Tp->ecgRate) % kEcgRing);
     if (ecg.tissue != tile.tissue || ecg.entry != entry) {
       ecg_flush(a, ecg, lane);
@@ -416,7 +416,7 @@ constexpr int min_ctas() { return MIXED ? 5 : CDB_FP64_MIN_CTAS; }
 // SLOT >= 0: the launch's reaction type is constant-memory slot SLOT and its
 // fits have the compiled shapes (fit_shapes.h); SLOT < 0: any slot (a.rt)
 // with run-time shapes.
-template <bool MIXED, int SLOT>
+template <bool MIXED, int SLOT, bool ECG>
 __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(StepArgs a)
 {
   constexpr int kBuf = stage_bytes<MIXED>();
@@ -433,10 +433,10 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
     if (t < a.nTiles) cur = a.tiles[t];
     for (; t < a.nTiles; t += stride) {
       if (t + stride < a.nTiles) nxt = a.tiles[t + stride];
-      step_tile<MIXED, SLOT>(a, cur, lane, nullptr, false, ecg);
+      step_tile<MIXED, SLOT, ECG>(a, cur, lane, nullptr, false, ecg);
       cur = nxt;
     }
-    ecg_flush(a, ecg, lane);
+    if (ECG) ecg_flush(a, ecg, lane);
     return;
   }
   // Buffer i holds tile t's inputs and the descriptor of tile t + stride,
@@ -463,48 +463,54 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
       if (tn + stride < a.nTiles) stage_desc(a.tiles + tn + stride, nextDesc, lane);
     }
     cp_async_commit();
-    step_tile<MIXED, SLOT>(a, cur, lane, mine + (it & 1) * kBuf, true, ecg);
+    step_tile<MIXED, SLOT, ECG>(a, cur, lane, mine + (it & 1) * kBuf, true, ecg);
     cur = nxt;
   }
   cp_async_wait_all();
-  ecg_flush(a, ecg, lane);
+  if (ECG) ecg_flush(a, ecg, lane);
 }
 
 // The compiled kernel of a slot when the type has the compiled fit shapes
-// (slot >= 0), else the generic kernel.
-template <bool MIXED>
-inline void (*step_kernel_for(int slot))(StepArgs)
+// (slot >= 0), else the generic kernel; with the ECG sensor compiled in or
+// out (only launches that hold a tissue with electrodes pay for it).
+template <bool MIXED, bool ECG>
+inline void (*step_kernel_of(int slot))(StepArgs)
 {
   static_assert(CDB_MAX_REACTION_TYPES == 6, "one compiled kernel per slot");
   switch (slot) {
-    case 0: return fused_step_kernel<MIXED, 0>;
-    case 1: return fused_step_kernel<MIXED, 1>;
-    case 2: return fused_step_kernel<MIXED, 2>;
-    case 3: return fused_step_kernel<MIXED, 3>;
-    case 4: return fused_step_kernel<MIXED, 4>;
-    case 5: return fused_step_kernel<MIXED, 5>;
-    default: return fused_step_kernel<MIXED, -1>;
+    case 0: return fused_step_kernel<MIXED, 0, ECG>;
+    case 1: return fused_step_kernel<MIXED, 1, ECG>;
+    case 2: return fused_step_kernel<MIXED, 2, ECG>;
+    case 3: return fused_step_kernel<MIXED, 3, ECG>;
+    case 4: return fused_step_kernel<MIXED, 4, ECG>;
+    case 5: return fused_step_kernel<MIXED, 5, ECG>;
+    default: return fused_step_kernel<MIXED, -1, ECG>;
   }
+}
+
+template <bool MIXED>
+inline void (*step_kernel_for(int slot, bool ecg))(StepArgs)
+{
+  return ecg ? step_kernel_of<MIXED, true>(slot) : step_kernel_of<MIXED, false>(slot);
 }
 
 // One step of one reaction type.
 template <bool MIXED>
-inline void launch_step(int slot, unsigned grid, cudaStream_t stream, const StepArgs& a)
+inline void launch_step(int slot, bool ecg, unsigned grid, cudaStream_t stream, const StepArgs& a)
 {
-  step_kernel_for<MIXED>(slot)<<<grid, kCta, 0, stream>>>(a);
+  step_kernel_for<MIXED>(slot, ecg)<<<grid, kCta, 0, stream>>>(a);
 }
 
 // CTAs of a slot's kernel that are resident on one SM at once (0 on error).
 template <bool MIXED>
-inline int resident_ctas(int slot)
+inline int resident_ctas(int slot, bool ecg)
 {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel_for<MIXED>(slot), kCta, 0) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel_for<MIXED>(slot, ecg), kCta, 0) != cudaSuccess)
     return 0;
   return n;
 }
 
-// After a launch batch of k steps: every tissue is k steps further.
 __global__ void advance_kernel(TissueDev* tissues, int nTissues, int k)
 {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;

@@ -155,14 +155,66 @@ def reactionFactory(db, name, dt, nCells, precision="fp64", device=0, generate=N
     return BetterTT06(params, nCells, dt, precision=precision, device=device)
 
 
+class CUDADiffusion:
+    """The reference's "cuda" 6-face Diffusion (CUDADiffusion,
+    elec/CUDADiffusion.cc:30-160): same interface as FGRDiffusion, its own
+    conductivity rule (cdb_diff6_*).  calc assigns dVm."""
+
+    def __init__(self, tissue, diffusionScale=None, device=0):
+        L = _lib.load()
+        self.nCells = tissue.n
+        self._diffusionScale = tissue.diffusion_scale if diffusionScale is None else diffusionScale
+        gid = np.ascontiguousarray(tissue.gid, dtype=np.int64)
+        sig = np.ascontiguousarray(tissue.sigma, dtype=np.float64)
+        h = ctypes.c_void_p()
+        _lib.check(L.cdb_diff6_create(device, tissue.nx, tissue.ny, tissue.nz, tissue.dx, tissue.dy, tissue.dz,
+                                      self.nCells, gid.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _lib.dptr(sig),
+                                      self._diffusionScale, ctypes.byref(h)))
+        self.h = h
+
+    def diffusionScale(self):
+        return self._diffusionScale
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.load().cdb_diff6_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def updateLocalVoltage(self, VmLocal):
+        _require_cuda(VmLocal)
+        _lib.check(_lib.load().cdb_diff6_update_local_voltage(self.h, _ptr(VmLocal), _stream()))
+
+    def updateRemoteVoltage(self, VmRemote):
+        if VmRemote is not None and VmRemote.numel() != 0:
+            raise ValueError("CUDADiffusion on one device has no remote cells")
+
+    def calc(self, dVm):
+        _require_cuda(dVm)
+        _lib.check(_lib.load().cdb_diff6_calc(self.h, _ptr(dVm), _stream()))
+
+    def face_sigma(self):
+        out = np.empty(self.nCells * 9)
+        _lib.check(_lib.load().cdb_diff6_get_face_sigma(self.h, _lib.dptr(out)))
+        return out.reshape(-1, 3, 3)
+
+
 def diffusionFactory(db, name, tissue, device=0):
     """diffusionFactory (elec/diffusionFactory.cc:37-101): method FGR (any
-    variant) or b200 -> FGRDiffusion; null -> None."""
+    variant) or b200 -> FGRDiffusion; cuda -> CUDADiffusion (6-face); null
+    -> None."""
     obj = db.find(name, "DIFFUSION")
     method = objectdb.get_str(obj, "method", "FGR")
     scale = objectdb.get_float(obj, "diffusionScale", 1.0)
     if method == "null":
         return None
+    if method == "cuda":
+        return CUDADiffusion(tissue, scale, device=device)
     if method not in ("FGR", "b200"):
         raise ValueError("DIFFUSION %s: method %s is not available on the B200 engine" % (name, method))
     return FGRDiffusion(tissue, scale, device=device)

@@ -138,6 +138,27 @@ cdb_status cdb_fgr_calc(cdb_fgr* d, double* dVm, void* stream);
 cdb_status cdb_fgr_get_weights(cdb_fgr* d, double* host19);
 cdb_status cdb_fgr_destroy(cdb_fgr* d);
 
+/* ------------------------------------------------------------------ */
+/* Diffusion plugin: the reference's "cuda" 6-face stencil.             */
+/* Replaces CUDADiffusion (elec/CUDADiffusion.cc:30-160, kernel         */
+/* diff_6face_v1, elec/CUDADiffusion_ker.cu:16-140) for users of        */
+/* method = cuda: each face carries the conductivity of the cell on its */
+/* + side (sigma area / h diffusionScale / volume), tangential terms    */
+/* only when their four nodes exist; dVm = sum of face flux             */
+/* differences (assigned).  Same cell and grid arguments as             */
+/* cdb_fgr_create; every given cell is present (cellType not checked,   */
+/* as in the reference).  cdb_diff6_get_face_sigma: host nCells x 9,    */
+/* the - face of axis i, component j at [9 c + 3 i + j].                */
+/* ------------------------------------------------------------------ */
+typedef struct cdb_diff6 cdb_diff6;
+cdb_status cdb_diff6_create(int device, int32_t nx, int32_t ny, int32_t nz, double dx, double dy, double dz,
+                            int64_t nCells, const int64_t* gid, const double* sigma6, double diffusionScale,
+                            cdb_diff6** out);
+cdb_status cdb_diff6_update_local_voltage(cdb_diff6* d, const double* Vm, void* stream);
+cdb_status cdb_diff6_calc(cdb_diff6* d, double* dVm, void* stream);
+cdb_status cdb_diff6_get_face_sigma(cdb_diff6* d, double* host9);
+cdb_status cdb_diff6_destroy(cdb_diff6* d);
+
 /* The FGR stencil for callers that cannot allocate device memory (code
  * inside another framework's allocator, or measurement code that must leave
  * the allocation state unchanged).  No counterpart in the reference.
