@@ -1,0 +1,54 @@
+"""The B200TT06 adapter (cardioid_b200/adapter/B200TT06.cc) inside the
+reference's own code: built as a dynamic reaction against the reference
+sources (oracle/ref/Makefile), loaded by the reference's reactionFactory
+(dlopen of the REACTION's method, elec/reactionFactory.cc:48-70), driven by
+the reference's ReactionManager, FGRDiffusionOMP, BoxStimulus and omp-loop
+integrator (oracle/ref/ref_driver.cc), and computing on the GPU through the
+C ABI.  Against the same simulation with the reference's own BetterTT06:
+FP64 max |dVm| <= 1e-6 mV after 300 steps, identical activation times."""
+import os
+
+import numpy as np
+import pytest
+
+from cardioid_b200 import engine, tissue
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ADAPTER = os.path.join(ROOT, "oracle", "_ref", "libb200tt06.so")
+
+
+def _built():
+    from oracle import refsim
+    return refsim.available() and os.path.exists(ADAPTER)
+
+
+@pytest.mark.skipif(not _built(), reason="oracle/_ref with the adapter not built")
+def test_adapter_in_reference_reaction_manager(cdb_lib):
+    from golden.make_golden import reference_sim
+    from oracle import refsim
+    t = tissue.box(10, 8, 6, dx=0.2, seed=17)
+    ref = reference_sim(t)           # compiles the shipped fits and the BetterTT06 objects
+    text = ""
+    for name, ct, fit in (("b200Endo", 0, "tt06Endo_fit"), ("b200Mid", 1, "tt06Mid_fit"), ("b200Epi", 2, "tt06Epi_fit")):
+        text += "%s REACTION { method = %s; cellTypes = %d; celltype = %d; fit = %s; }\n" % (name, ADAPTER, 100 + ct,
+                                                                                          ct, fit)
+    refsim.compile_once("b200-adapter", text)
+    prefix = refsim.unique_prefix()
+    refsim.compile_objects(tissue.stimulus_objects_text(t.stimuli, prefix=prefix))
+    gpu = refsim.RefSim(["b200Endo", "b200Mid", "b200Epi"], ["%s%d" % (prefix, i) for i in range(len(t.stimuli))],
+                        (t.nx, t.ny, t.nz), (t.dx, t.dy, t.dz), t.gid, t.cell_type, t.sigma, 0.02, t.diffusion_scale)
+    # both start from the reactions' own initial Vm (initializeMembraneVoltage)
+    np.testing.assert_array_equal(gpu.vm(), ref.vm())
+    ref.set_vm(t.vm0)
+    gpu.set_vm(t.vm0)
+    for _ in range(3):
+        ref.step(100)
+        gpu.step(100)
+    assert np.abs(gpu.vm() - ref.vm()).max() <= 1e-6
+    np.testing.assert_array_equal(gpu.activation(), ref.activation())
+    assert (ref.activation() > 0).any()
+    for name in ("Ca_i", "m", "h"):
+        r = ref.state(name)
+        assert np.abs(gpu.state(name) - r).max() <= 1e-8 * max(1e-12, np.abs(r).max())
