@@ -271,3 +271,26 @@ def test_mixed_precision_errors_vs_fp64_oracle(cdb_lib, oracle_port, fits002):
         a_o, a_m = apd90(tr_o[:, j], times), apd90(tr_m[:, j], times)
         assert len(a_o) == len(a_m) and len(a_o) >= 1
         assert np.abs(a_o - a_m).max() <= APD_TOL_MIXED
+
+
+def test_full_size_box_mixed_vs_fp64_and_repeatable(cdb_lib):
+    """At the benchmark's size (256^3, three transmural types, S1 pacing):
+    two FP64 runs agree bit for bit (no order-dependent reductions in the
+    step), and the mixed run's activation times stay within 0.5 ms of FP64
+    over the first 5 ms of the wave."""
+    t = tissue.box(256, 256, 256, period=500.0)
+    steps = 250
+    acts, vms = {}, {}
+    for run, precision in (("a", "fp64"), ("b", "fp64"), ("m", "mixed")):
+        with eng_mod.Engine(DT, precision=precision) as e:
+            rx, _ = eng_mod.transmural_setup(e, t, DT)
+            tid = e.add_tissue(t, rx)
+            e.step(steps)
+            acts[run], vms[run] = e.read_activation(tid), e.read_vm(tid)
+    np.testing.assert_array_equal(vms["a"], vms["b"])
+    np.testing.assert_array_equal(acts["a"], acts["b"])
+    a, m = acts["a"], acts["m"]
+    assert (a > 0).sum() > 100_000
+    both = (a > 0) & (m > 0)
+    assert ((a > 0) != (m > 0)).mean() < 1e-3
+    assert np.abs(a[both] - m[both]).max() <= ACT_TOL_MIXED
