@@ -252,12 +252,14 @@ def run_ours(args):
     peak, peak_src = read_peaks()
     results = {}
     precs = ("fp64", "mixed") if args.precision == "both" else (args.precision,)
+    finals = {}
     for prec in precs:
         with engine.Engine(DT, precision=prec, device=local) as e:
             rx, _ = engine.transmural_setup(e, t, DT)
             e.add_tissue(t, rx)
             ms, launches, clocks = time_engine(e, args.steps, args.warmup, world, local)
             ms = max_over_ranks(ms, world, local)
+            finals[prec] = (e.read_vm(0), e.read_activation(0), e.time(0)[0])
             per_launch_s = ms / 1e3 / args.steps
             achieved = ALGO_BYTES[prec] * n / per_launch_s / 1e9
             traffic_pc = read_traffic(prec)
@@ -297,6 +299,13 @@ def run_ours(args):
                   flush=True)
         return
     m, f = results["mixed"], results["fp64"]
+    (vf, af, sf), (vm_, am, sm_) = finals["fp64"], finals["mixed"]
+    both = (af > 0) & (am > 0)
+    errors = {"steps": int(sf), "max_abs_dvm_mV": float(np.abs(vm_ - vf).max()),
+              "activated_fp64": int((af > 0).sum()), "activated_mixed": int((am > 0).sum()),
+              "activation_max_err_ms": float(np.abs(af[both] - am[both]).max()) if both.any() else None,
+              "apd90": "beats last 300 ms, past this window; tests/test_engine_gpu.py checks APD90 on a full beat"}
+    plain = time_plain_fp64(t, args, local) if world == 1 and not args.no_plain else None
     line = {
         "metric": METRIC, "value": m["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -313,6 +322,9 @@ def run_ours(args):
         "fp64": {"value": f["value"], "ms_per_step": f["ms_per_step"], "roofline": f["roofline"],
                  "dtype": "f64"},
         "mixed_over_fp64": m["value"] / f["value"],
+        "mixed_vs_fp64": errors,
+        "plain_fp64": plain,
+        "mixed_over_plain_fp64": (m["value"] / plain["value"]) if plain else None,
         "e2e": results["e2e"],
         "gpu_launches": m["gpu_launches"],
         "clocks": m["clocks"],
@@ -412,6 +424,49 @@ def run_serve(args):
                           "%d steps each at dt %g" % (args.jobs, args.rate, args.job_steps, DT), **out}), flush=True)
 
 
+def time_plain_fp64(t, args, local):
+    """The plain FP64 GPU path: the reference's split loop on the drop-in
+    plugins (elec/simulationLoop.cc:183-231), one Reaction::calc per
+    reaction type (cdb_reaction_calc), Diffusion::updateLocalVoltage and
+    calc (cdb_fgr_*), then iStim and Vm += dt (dVmR + dVmD + iStim) as
+    tensor operations; Vm crosses HBM several times per step."""
+    import torch
+    from cardioid_b200 import engine, plugins
+    dev = "cuda:%d" % local
+    params = [engine.default_params(c, DT) for c in (0, 1, 2)]
+    ct = torch.from_numpy(np.asarray(t.cell_type) - 100).to(dev)
+    idx = [torch.nonzero(ct == c).flatten().to(torch.int32) for c in (0, 1, 2)]
+    rx = [plugins.BetterTT06(params[c], idx[c].numel(), DT) for c in (0, 1, 2)]
+    fgr = plugins.FGRDiffusion(t)
+    vm = torch.from_numpy(t.vm0.copy()).to(dev)
+    dvr, dvd, ist = torch.zeros_like(vm), torch.zeros_like(vm), torch.zeros_like(vm)
+    x = torch.from_numpy(np.asarray(t.tuples()[0])).to(dev)
+    face = (x > t.stimuli[0].xMin) & (x < t.stimuli[0].xMax)
+    amp = t.stimuli[0].amplitude
+
+    def step(n):
+        for _ in range(n):
+            ist.zero_()
+            ist.masked_fill_(face, amp)          # on at t < 1 ms of the first beat only; the cost is the same
+            for c in (0, 1, 2):
+                rx[c].calc(DT, idx[c], vm, ist, dvr)
+            fgr.updateLocalVoltage(vm)
+            fgr.calc(dvd)
+            vm.add_(DT * (dvr + dvd + ist))
+    steps = min(args.steps, 200)
+    step(args.warmup)
+    torch.cuda.synchronize(local)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    step(steps)
+    s1.record()
+    s1.synchronize()
+    ms = s0.elapsed_time(s1)
+    return {"value": t.n * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps, "dtype": "f64",
+            "path": "split loop on the plugins: 3 x cdb_reaction_calc + cdb_fgr_update_local_voltage + cdb_fgr_calc "
+                    "+ stimulus and Vm update as tensor ops (CUDA events, default stream)"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -451,6 +506,7 @@ def main():
     ap.add_argument("--precision", choices=["both", "fp64", "mixed"], default="both",
                     help="profiling runs: time one precision only (no headline line)")
     ap.add_argument("--no-e2e", action="store_true", help="profiling runs: skip the end-to-end loop")
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 plugin path")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

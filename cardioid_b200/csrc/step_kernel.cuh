@@ -82,6 +82,14 @@ static_assert(sizeof(WarpTile) == 32, "tile descriptors are copied as two 16-byt
 constexpr int kEcgRing = 1024;
 constexpr int kEcgMaxPoints = 32;
 
+// A lane's running min/max of Vm for one tissue over the warp's tiles of a
+// min/max step; the warp reduces it and adds it to the tissue's sensor when
+// the tissue changes and at the end (two atomics per warp, not per tile).
+struct MinMaxAcc {
+  double lo, hi;
+  int tissue;
+};
+
 // A warp's running ECG sum (lane j: electrode j) for one tissue and one
 // evaluation entry, added to the trace when either changes.
 struct EcgAcc {
@@ -239,6 +247,25 @@ __device__ __forceinline__ void stage_tile(const StepArgs& a, const WarpTile& ti
   warp_copy(buf + vrel_offset<MIXED>(), (const unsigned char*)(Tp->vrel + b * kBlk), kBlk * 4, lane);
 }
 
+__device__ __forceinline__ void minmax_flush(const StepArgs& a, MinMaxAcc& acc, int lane)
+{
+  if (acc.tissue >= 0) {
+    double lo = acc.lo, hi = acc.hi;
+    for (int o = 16; o > 0; o >>= 1) {
+      lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane == 0) {
+      unsigned long long* mm = a.tissues[acc.tissue].minmax;
+      atomicMin(mm, ordered_bits(lo));
+      atomicMax(mm + 1, ordered_bits(hi));
+    }
+  }
+  acc.tissue = -1;
+  acc.lo = __longlong_as_double(0x7ff0000000000000ll);
+  acc.hi = -__longlong_as_double(0x7ff0000000000000ll);
+}
+
 __device__ __forceinline__ void ecg_flush(const StepArgs& a, EcgAcc& acc, int lane)
 {
   if (acc.tissue >= 0) {
@@ -253,7 +280,7 @@ __device__ __forceinline__ void ecg_flush(const StepArgs& a, EcgAcc& acc, int la
 // from buf; otherwise straight from global memory.
 template <bool MIXED, int SLOT, bool ECG>
 __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& tile, int lane, const unsigned char* buf,
-                                          bool staged, EcgAcc& ecg)
+                                          bool staged, EcgAcc& ecg, MinMaxAcc& mm)
 {
   constexpr bool SPEC = SLOT >= 0;
   const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
@@ -361,15 +388,13 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
     }
   }
   if (a.minmax) {
-    double lo = active ? vnew : __longlong_as_double(0x7ff0000000000000ll);
-    double hi = active ? vnew : -__longlong_as_double(0x7ff0000000000000ll);
-    for (int o = 16; o > 0; o >>= 1) {
-      lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    if (mm.tissue != tile.tissue) {
+      minmax_flush(a, mm, lane);
+      mm.tissue = tile.tissue;
     }
-    if (lane == 0) {
-      atomicMin(Tp->minmax, ordered_bits(lo));
-      atomicMax(Tp->minmax + 1, ordered_bits(hi));
+    if (active) {
+      mm.lo = fmin(mm.lo, vnew);
+      mm.hi = fmax(mm.hi, vnew);
     }
   }
   // ECG (ECGSensor::eval / calcEcg, elec/ECGSensor.cc:231-320 and
@@ -430,13 +455,15 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
     // the next tile's descriptor is in flight while this tile computes
     WarpTile cur, nxt;
     EcgAcc ecg{0.0, -1, 0};
+    MinMaxAcc mm{__longlong_as_double(0x7ff0000000000000ll), -__longlong_as_double(0x7ff0000000000000ll), -1};
     if (t < a.nTiles) cur = a.tiles[t];
     for (; t < a.nTiles; t += stride) {
       if (t + stride < a.nTiles) nxt = a.tiles[t + stride];
-      step_tile<MIXED, SLOT, ECG>(a, cur, lane, nullptr, false, ecg);
+      step_tile<MIXED, SLOT, ECG>(a, cur, lane, nullptr, false, ecg, mm);
       cur = nxt;
     }
     if (ECG) ecg_flush(a, ecg, lane);
+    if (a.minmax) minmax_flush(a, mm, lane);
     return;
   }
   // Buffer i holds tile t's inputs and the descriptor of tile t + stride,
@@ -451,6 +478,7 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
   cp_async_commit();
   WarpTile cur = t < a.nTiles ? a.tiles[t] : WarpTile{};
   EcgAcc ecg{0.0, -1, 0};
+  MinMaxAcc mm{__longlong_as_double(0x7ff0000000000000ll), -__longlong_as_double(0x7ff0000000000000ll), -1};
   for (int it = 0; t < a.nTiles; ++it, t += stride) {
     const int tn = t + stride;
     WarpTile* mineDesc = (it & 1) ? desc1 : desc0;        // descriptor of tile tn, copied with tile t
@@ -463,11 +491,12 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
       if (tn + stride < a.nTiles) stage_desc(a.tiles + tn + stride, nextDesc, lane);
     }
     cp_async_commit();
-    step_tile<MIXED, SLOT, ECG>(a, cur, lane, mine + (it & 1) * kBuf, true, ecg);
+    step_tile<MIXED, SLOT, ECG>(a, cur, lane, mine + (it & 1) * kBuf, true, ecg, mm);
     cur = nxt;
   }
   cp_async_wait_all();
   if (ECG) ecg_flush(a, ecg, lane);
+  if (a.minmax) minmax_flush(a, mm, lane);
 }
 
 // The compiled kernel of a slot when the type has the compiled fit shapes
