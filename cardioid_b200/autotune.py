@@ -1,6 +1,6 @@
 """Autotuner for the fused step's launch shape.
 
-For each candidate (shared-memory staging on/off, CTAs per SM of the
+For each candidate (shared-memory staging mode, CTAs per SM of the
 persistent grid) it times a few steps of the engine's current tissues with
 CUDA events on the engine's stream and keeps the fastest.  Timing advances
 the tissues: run it during warm-up, or on a scratch engine holding a tissue
@@ -8,7 +8,7 @@ of the same shape.
 """
 import itertools
 
-STAGE_MODES = (0, 1)
+STAGE_MODES = (0, 1, 2)    # direct loads, cp.async, bulk copies
 CTAS_PER_SM = (0, 4, 8)     # 0: as many as are resident
 
 

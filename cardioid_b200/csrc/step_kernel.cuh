@@ -108,7 +108,8 @@ struct StepArgs {
   double dt;
   int k;                      // step within the launch batch
   int minmax;                 // reduce min/max this step
-  int stage;                  // 1: stage the next tile through shared memory
+  int stage;                  // 1: stage the next tile through shared memory (cp.async), 2: with bulk copies
+  int* err;                   // set to CDB_TIMEOUT when a bounded wait gives up
 };
 
 __constant__ TT06Scalars c_scal[CDB_MAX_REACTION_TYPES];
@@ -274,6 +275,84 @@ __device__ __forceinline__ void ecg_flush(const StepArgs& a, EcgAcc& acc, int la
   }
   acc.tissue = -1;
   acc.v = 0.0;
+}
+
+// ---- bulk (TMA) staging: one lane issues cp.async.bulk copies of the
+// tile's contiguous blocks, completing on the buffer's mbarrier ----
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity)
+{
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes, unsigned long long* bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Bounded wait for a buffer's copies (every lane): false after about 2^20
+// polls, each of which the hardware may suspend for a while.
+constexpr int kWaitPolls = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
+{
+  for (int i = 0; i < kWaitPolls; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Lane 0: copies a tile's state block, weight block (mixed) and voxel
+// offsets, and the descriptor of the tile after it (when there is one),
+// into buf, all completing on bar.
+template <bool MIXED>
+__device__ __forceinline__ void stage_tile_bulk(const StepArgs& a, const WarpTile& tile, unsigned char* buf,
+                                                const WarpTile* nextDesc, WarpTile* descDst, unsigned long long* bar)
+{
+  const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
+  const int64_t b = tile.first / kBlk;
+  unsigned bytes = kBlk * 4 + (nextDesc ? 32u : 0u);
+  int wr = 0;
+  if (MIXED) {
+    bytes += kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4;
+    if (Tp->scale != 0.0) wr = weight_rows(Tp->cls, true);
+    bytes += wr * kBlk * 4;
+  } else {
+    bytes += kRows64 * kBlk * 8;
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // after this warp's reads of buf
+  mbar_expect_tx(bar, bytes);
+  if (MIXED) {
+    bulk_copy(buf, Tp->s64 + b * kRowsMixed64 * kBlk, kRowsMixed64 * kBlk * 8, bar);
+    bulk_copy(buf + kRowsMixed64 * kBlk * 8, Tp->s32 + b * kRowsMixed32 * kBlk, kRowsMixed32 * kBlk * 4, bar);
+    if (wr)
+      bulk_copy(buf + kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4, (const float*)Tp->w + b * wr * kBlk,
+                wr * kBlk * 4, bar);
+  } else {
+    bulk_copy(buf, Tp->s64 + b * kRows64 * kBlk, kRows64 * kBlk * 8, bar);
+  }
+  bulk_copy(buf + vrel_offset<MIXED>(), Tp->vrel + b * kBlk, kBlk * 4, bar);
+  if (nextDesc) bulk_copy(descDst, nextDesc, 32, bar);
 }
 
 // One tile.  With `staged` the tile's state (and mixed weights) are read
@@ -445,7 +524,7 @@ template <bool MIXED, int SLOT, bool ECG>
 __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(StepArgs a)
 {
   constexpr int kBuf = stage_bytes<MIXED>();
-  __shared__ __align__(16) unsigned char smem[kWarpsPerCta * 2 * kBuf];
+  __shared__ __align__(16) unsigned char smem[kWarpsPerCta * 2 * kBuf + kWarpsPerCta * 2 * 8];
   const int lane = threadIdx.x & 31;
   const int warpInCta = threadIdx.x >> 5;
   unsigned char* mine = smem + warpInCta * 2 * kBuf;
@@ -460,6 +539,46 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
     for (; t < a.nTiles; t += stride) {
       if (t + stride < a.nTiles) nxt = a.tiles[t + stride];
       step_tile<MIXED, SLOT, ECG>(a, cur, lane, nullptr, false, ecg, mm);
+      cur = nxt;
+    }
+    if (ECG) ecg_flush(a, ecg, lane);
+    if (a.minmax) minmax_flush(a, mm, lane);
+    return;
+  }
+  if (a.stage == 2) {
+    // Bulk copies: lane 0 issues, for tile t + stride, cp.async.bulk copies
+    // of its contiguous blocks (and of the descriptor after it) into the
+    // other buffer while the warp computes tile t; every lane waits on the
+    // buffer's mbarrier, phase (iteration / 2) & 1.
+    unsigned long long* bars = (unsigned long long*)(smem + kWarpsPerCta * 2 * kBuf) + warpInCta * 2;
+    WarpTile* const desc0 = (WarpTile*)(mine + vrel_offset<MIXED>() + kBlk * 4);
+    WarpTile* const desc1 = (WarpTile*)(mine + kBuf + vrel_offset<MIXED>() + kBlk * 4);
+    if (lane == 0) {
+      mbar_init(bars, 1);
+      mbar_init(bars + 1, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    EcgAcc ecg{0.0, -1, 0};
+    MinMaxAcc mm{__longlong_as_double(0x7ff0000000000000ll), -__longlong_as_double(0x7ff0000000000000ll), -1};
+    WarpTile cur = t < a.nTiles ? a.tiles[t] : WarpTile{};
+    if (t < a.nTiles && lane == 0)
+      stage_tile_bulk<MIXED>(a, cur, mine, t + stride < a.nTiles ? a.tiles + t + stride : nullptr, desc0, bars);
+    for (int it = 0; t < a.nTiles; ++it, t += stride) {
+      const int tn = t + stride;
+      const int bi = it & 1;
+      if (!__all_sync(0xffffffffu, mbar_wait(bars + bi, (it >> 1) & 1))) {
+        if (lane == 0) atomicExch(a.err, (int)CDB_TIMEOUT);
+        mbar_wait(bars + bi, (it >> 1) & 1);    // let its copies land before the warp leaves
+        return;
+      }
+      __syncwarp();           // every lane is past the wait and done with the other buffer
+      const WarpTile nxt = tn < a.nTiles ? *(bi ? desc1 : desc0) : WarpTile{};
+      if (tn < a.nTiles && lane == 0)
+        stage_tile_bulk<MIXED>(a, nxt, mine + (bi ^ 1) * kBuf,
+                               tn + stride < a.nTiles ? a.tiles + tn + stride : nullptr, bi ? desc0 : desc1,
+                               bars + (bi ^ 1));
+      step_tile<MIXED, SLOT, ECG>(a, cur, lane, mine + bi * kBuf, true, ecg, mm);
       cur = nxt;
     }
     if (ECG) ecg_flush(a, ecg, lane);

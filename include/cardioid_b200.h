@@ -216,7 +216,9 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
 cdb_status cdb_engine_remove_tissue(cdb_engine* e, int32_t id);
 /* Advances every tissue by nSteps steps of dt (one fused kernel per step). */
 cdb_status cdb_engine_step(cdb_engine* e, int32_t nSteps);
-/* Blocks until the engine's stream is idle. */
+/* Blocks until the engine's stream is idle; CDB_TIMEOUT if a bounded wait
+ * inside the step gave up since the last call (the affected steps are
+ * incomplete). */
 cdb_status cdb_engine_sync(cdb_engine* e);
 /* Number of steps a tissue has taken and its time (ms, accumulated as
  * time += dt like the reference). */
@@ -266,10 +268,11 @@ cdb_status cdb_diag_div64(int device, int64_t n, const double* a, const double* 
 
 /* Launch tuning of the step kernel (no counterpart in the reference):
  * stage 1 = each warp copies its next tile's state (mixed: and weights)
- * into shared memory with cp.async while it computes the current one, 0 =
- * direct loads; ctasPerSm sizes the persistent grid (SMs x ctasPerSm CTAs
+ * into shared memory with cp.async while it computes the current one, 2 =
+ * the same with bulk (TMA) copies completing on an mbarrier, 0 = direct
+ * loads; ctasPerSm sizes the persistent grid (SMs x ctasPerSm CTAs
  * of 128 threads), 0 = as many CTAs as are resident on an SM at once.
- * Defaults: stage 1 for CDB_MIXED, 0 for CDB_FP64, ctasPerSm 0;
+ * Defaults: stage 2 for CDB_MIXED, 0 for CDB_FP64, ctasPerSm 0;
  * cardioid_b200.autotune picks them by timing. */
 cdb_status cdb_engine_set_tuning(cdb_engine* e, int32_t stage, int32_t ctasPerSm);
 cdb_status cdb_engine_get_tuning(cdb_engine* e, int32_t* stage, int32_t* ctasPerSm);

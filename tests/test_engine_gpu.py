@@ -294,3 +294,23 @@ def test_full_size_box_mixed_vs_fp64_and_repeatable(cdb_lib):
     both = (a > 0) & (m > 0)
     assert ((a > 0) != (m > 0)).mean() < 1e-3
     assert np.abs(a[both] - m[both]).max() <= ACT_TOL_MIXED
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_staging_modes_agree(cdb_lib, fits002, precision):
+    """Direct loads (0), per-lane cp.async staging (1) and bulk-copy staging
+    on mbarriers (2) compute the same bits, on a mix of tissue classes and
+    with several tiles per warp (small grid)."""
+    ts = [tissue.box(40, 33, 9, seed=8), tissue.box(300, 1, 1, seed=9), _masked(13, 12, 11, seed=10)]
+    out = {}
+    for stage in (0, 1, 2):
+        with _engine(fits002, precision=precision) as e:
+            e.set_tuning(stage, 1)
+            ids = [e.add_tissue(t, _reaction_ids(t)) for t in ts]
+            e.step(60)
+            e.sync()
+            out[stage] = [(e.read_vm(i), e.read_states(i), e.read_activation(i)) for i in ids]
+    for stage in (1, 2):
+        for a, b in zip(out[0], out[stage]):
+            for x, y in zip(a, b):
+                np.testing.assert_array_equal(x, y)
