@@ -176,7 +176,9 @@ struct Engine {
     for (size_t c = 0; c < clocks.size(); ++c) {
       std::vector<double>& t = clocks[c].times;
       if ((int64_t)t.size() >= need[c]) continue;
-      const int64_t want = std::max<int64_t>(need[c], (int64_t)t.size() * 2);
+      // at least 2^16 steps at a time: a re-upload drains the stream and
+      // re-captures the step graph, so it must stay rare in long runs
+      const int64_t want = std::max<int64_t>(need[c], std::max<int64_t>((int64_t)t.size() * 2, int64_t(1) << 16));
       t.reserve(want);
       while ((int64_t)t.size() < want) t.push_back(t.back() + cfg.dt);
       grew = true;
