@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -33,6 +34,7 @@
 
 #include "common.cuh"
 #include "fgr_device.cuh"
+#include "reaction_slot.h"
 #include "step_kernel.cuh"
 
 namespace cdb {
@@ -85,29 +87,62 @@ struct HostTissue {
 };
 
 // Constant-memory reaction slots are a per-device resource shared by every
-// engine of the process; each engine takes slots as it registers reaction
-// types and gives them back when destroyed.
+// engine and plugin reaction of the process.  Registrations with identical
+// content (scalars, fit shape, coefficient pool) share a slot, reference
+// counted; a slot is uploaded when it is taken and reused once released.
+struct SlotEntry {
+  int refs = 0;
+  bool spec = false;                 // pool packed for the compiled fit shapes
+  std::vector<unsigned char> key;    // the uploaded content
+};
 std::mutex g_slot_mutex;
-std::map<int, std::vector<bool>> g_slot_used;
+std::map<int, std::vector<SlotEntry>> g_slots;
 
-int acquire_slot(int device)
+// The slot holding this content (uploaded when new); -1 when every slot is
+// taken (err stays cudaSuccess) or the upload failed (err set).  The
+// caller has made `device` current.
+int acquire_slot(int device, const TT06Scalars& scal, const FitShape& shape, const std::vector<double>& pool,
+                 bool spec, cudaError_t& err)
 {
+  std::vector<unsigned char> key(sizeof(scal) + sizeof(shape) + pool.size() * sizeof(double) + 1);
+  unsigned char* k = key.data();
+  std::memcpy(k, &scal, sizeof(scal));
+  std::memcpy(k + sizeof(scal), &shape, sizeof(shape));
+  std::memcpy(k + sizeof(scal) + sizeof(shape), pool.data(), pool.size() * sizeof(double));
+  key.back() = spec ? 1 : 0;
   std::lock_guard<std::mutex> lock(g_slot_mutex);
-  std::vector<bool>& used = g_slot_used[device];
-  used.resize(CDB_MAX_REACTION_TYPES, false);
+  std::vector<SlotEntry>& used = g_slots[device];
+  used.resize(CDB_MAX_REACTION_TYPES);
   for (int s = 0; s < CDB_MAX_REACTION_TYPES; ++s)
-    if (!used[s]) {
-      used[s] = true;
+    if (used[s].refs > 0 && used[s].key == key) {
+      ++used[s].refs;
       return s;
     }
+  for (int s = 0; s < CDB_MAX_REACTION_TYPES; ++s) {
+    if (used[s].refs > 0) continue;
+    const std::vector<float> pool32(pool.begin(), pool.end());
+    err = cudaMemcpyToSymbol(c_scal, &scal, sizeof(scal), s * sizeof(TT06Scalars));
+    if (err == cudaSuccess) err = cudaMemcpyToSymbol(c_shape, &shape, sizeof(shape), s * sizeof(FitShape));
+    if (err == cudaSuccess)
+      err = cudaMemcpyToSymbol(c_coef64, pool.data(), pool.size() * sizeof(double),
+                               (size_t)s * kFitPoolPerType * sizeof(double));
+    if (err == cudaSuccess)
+      err = cudaMemcpyToSymbol(c_coef32, pool32.data(), pool32.size() * sizeof(float),
+                               (size_t)s * kFitPoolPerType * sizeof(float));
+    if (err != cudaSuccess) return -1;
+    used[s].refs = 1;
+    used[s].spec = spec;
+    used[s].key = std::move(key);
+    return s;
+  }
   return -1;
 }
 
 void release_slot(int device, int slot)
 {
   std::lock_guard<std::mutex> lock(g_slot_mutex);
-  std::vector<bool>& used = g_slot_used[device];
-  if (slot >= 0 && slot < (int)used.size()) used[slot] = false;
+  std::vector<SlotEntry>& used = g_slots[device];
+  if (slot >= 0 && slot < (int)used.size() && used[slot].refs > 0) --used[slot].refs;
 }
 
 struct Engine {
@@ -342,6 +377,74 @@ struct Engine {
   }
   int64_t graphLaunches = 0;
 };
+
+// ---- plugin reactions on constant-memory slots (reaction_slot.h) ----
+
+// One cell per thread in the plugin's layout (state rows of pitch n, Vm and
+// dVm through the index array), the slot's scalars and coefficients with
+// the compiled fit shapes: the same arithmetic as the fused step's reaction.
+template <bool MIXED, int SLOT>
+__global__ void __launch_bounds__(kCta, min_ctas<MIXED>())
+    reaction_slot_kernel(int64_t n, double dt, const int32_t* __restrict__ index, const double* __restrict__ Vm,
+                         double* __restrict__ dVm, double* __restrict__ s64, float* __restrict__ s32)
+{
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t e = index[i];
+  const double V = Vm[e];
+  const BlockScale none{1.0, 1.0, 1.0};
+  const double* c64 = c_coef64 + SLOT * kFitPoolPerType;
+  if (MIXED) {
+    IOMixed io{s64 + i, s32 + i, n};
+    SpecFits fits{c64, c_coef32 + SLOT * kFitPoolPerType};
+    dVm[e] = (double)tt06_step_mixed(c_scal[SLOT], none, fits, (float)dt, V, io);
+  } else {
+    IO64 io{s64 + i, n};
+    SpecFits fits{c64, nullptr};
+    dVm[e] = tt06_step(c_scal[SLOT], none, fits, dt, V, io);
+  }
+}
+
+template <bool MIXED>
+cudaError_t launch_reaction_slot(int slot, int64_t n, double dt, const int32_t* index, const double* Vm, double* dVm,
+                                 double* s64, float* s32, cudaStream_t stream)
+{
+  static_assert(CDB_MAX_REACTION_TYPES == 6, "one compiled kernel per slot");
+  void (*k)(int64_t, double, const int32_t*, const double*, double*, double*, float*) = nullptr;
+  switch (slot) {
+    case 0: k = reaction_slot_kernel<MIXED, 0>; break;
+    case 1: k = reaction_slot_kernel<MIXED, 1>; break;
+    case 2: k = reaction_slot_kernel<MIXED, 2>; break;
+    case 3: k = reaction_slot_kernel<MIXED, 3>; break;
+    case 4: k = reaction_slot_kernel<MIXED, 4>; break;
+    case 5: k = reaction_slot_kernel<MIXED, 5>; break;
+    default: return cudaErrorInvalidValue;
+  }
+  k<<<(unsigned)((n + kCta - 1) / kCta), kCta, 0, stream>>>(n, dt, index, Vm, dVm, s64, s32);
+  return cudaGetLastError();
+}
+
+int reaction_slot_acquire(int device, const cdb_tt06_params& params, const cdb_fit* fits)
+{
+  FitShape shape{};
+  std::vector<double> pool(kFitPoolPerType, 0.0);
+  std::string err;
+  if (!pack_fits(fits, shape, pool.data(), kFitPoolPerType, err)) return -1;
+  if (!pack_fits_spec(fits, pool.data(), kFitPoolPerType)) return -1;
+  if (cudaSetDevice(device) != cudaSuccess) return -1;
+  cudaError_t up = cudaSuccess;
+  const int slot = acquire_slot(device, to_scalars(params), shape, pool, true, up);
+  return up == cudaSuccess ? slot : -1;
+}
+
+void reaction_slot_release(int device, int slot) { release_slot(device, slot); }
+
+cudaError_t reaction_slot_calc(int slot, bool mixed, int64_t n, double dt, const int32_t* index, const double* Vm,
+                               double* dVm, double* s64, float* s32, cudaStream_t stream)
+{
+  return mixed ? launch_reaction_slot<true>(slot, n, dt, index, Vm, dVm, s64, s32, stream)
+               : launch_reaction_slot<false>(slot, n, dt, index, Vm, dVm, s64, s32, stream);
+}
 
 }  // namespace cdb
 
@@ -579,21 +682,17 @@ cdb_status cdb_engine_add_reaction(cdb_engine* e, const cdb_tt06_params* params,
   const bool specialised = pack_fits_spec(fits, pool.data(), kFitPoolPerType);
   const TT06Scalars scal = to_scalars(*params);
   CDB_CUDA(cudaSetDevice(E.cfg.device));
-  const int slot = acquire_slot(E.cfg.device);
+  CDB_CUDA(cudaStreamSynchronize(E.stream));
+  cudaError_t up = cudaSuccess;
+  const int slot = acquire_slot(E.cfg.device, scal, shape, pool, specialised, up);
+  CDB_CUDA(up);
   CDB_CHECK(slot >= 0, CDB_INVALID_ARG,
             "every constant-memory reaction slot of this device is in use (at most " +
-                std::to_string(CDB_MAX_REACTION_TYPES) + " reaction types across the process's engines)");
+                std::to_string(CDB_MAX_REACTION_TYPES) +
+                " distinct reaction types across the process's engines and plugin reactions)");
   E.slots[E.nTypes] = slot;
   E.spec[slot] = specialised;
-  E.nTypes += 1;   // the engine owns the slot from here on; destroy releases it
-  std::vector<float> pool32(pool.begin(), pool.end());
-  CDB_CUDA(cudaStreamSynchronize(E.stream));
-  CDB_CUDA(cudaMemcpyToSymbol(c_scal, &scal, sizeof(scal), slot * sizeof(TT06Scalars)));
-  CDB_CUDA(cudaMemcpyToSymbol(c_shape, &shape, sizeof(shape), slot * sizeof(FitShape)));
-  CDB_CUDA(cudaMemcpyToSymbol(c_coef64, pool.data(), pool.size() * sizeof(double),
-                              (size_t)slot * kFitPoolPerType * sizeof(double)));
-  CDB_CUDA(cudaMemcpyToSymbol(c_coef32, pool32.data(), pool32.size() * sizeof(float),
-                              (size_t)slot * kFitPoolPerType * sizeof(float)));
+  E.nTypes += 1;   // the engine holds the slot from here on; destroy releases it
   *id = E.nTypes - 1;
   return CDB_OK;
 }

@@ -16,6 +16,7 @@
 
 #include "common.cuh"
 #include "fgr_device.cuh"
+#include "reaction_slot.h"
 #include "tt06_step.cuh"
 
 namespace cdb {
@@ -135,6 +136,8 @@ struct cdb_reaction {
   TT06Scalars p{};
   FitShape sh{};
   Buf coef64, coef32, s64, s32;
+  int slot = -1;   // constant-memory slot with the compiled fit shapes, or -1: the generic kernel
+  ~cdb_reaction() { reaction_slot_release(device, slot); }
 };
 
 struct cdb_fgr {
@@ -169,6 +172,7 @@ cdb_status cdb_reaction_create(int device, cdb_precision precision, const cdb_tt
   CDB_CUDA(r->coef32.alloc(pool32.size() * 4));
   CDB_CUDA(cudaMemcpy(r->coef64.p, pool.data(), pool.size() * 8, cudaMemcpyHostToDevice));
   CDB_CUDA(cudaMemcpy(r->coef32.p, pool32.data(), pool32.size() * 4, cudaMemcpyHostToDevice));
+  r->slot = reaction_slot_acquire(device, *params, fits);
   const int64_t n = std::max<int64_t>(nCells, 1);
   if (precision == CDB_MIXED) {
     CDB_CUDA(r->s64.alloc(n * 5 * 8));
@@ -202,6 +206,11 @@ cdb_status cdb_reaction_calc(cdb_reaction* r, double dt, const int32_t* indexArr
   CDB_CHECK(dt == r->dt, CDB_INVALID_ARG, "dt differs from the dt the fits were made for");
   CDB_CUDA(cudaSetDevice(r->device));
   if (r->n == 0) return CDB_OK;
+  if (r->slot >= 0) {
+    CDB_CUDA(reaction_slot_calc(r->slot, r->prec == CDB_MIXED, r->n, dt, indexArray, Vm, dVm, r->s64.as<double>(),
+                                r->s32.as<float>(), (cudaStream_t)stream));
+    return CDB_OK;
+  }
   ReactionArgs a;
   a.p = r->p;
   a.sh = r->sh;

@@ -98,6 +98,13 @@ double cdb_fit_eval(const cdb_fit* fit, double x);
 /* ------------------------------------------------------------------ */
 typedef struct cdb_reaction cdb_reaction;
 
+/* A reaction whose fits have the compiled shapes (the shipped fit files'
+ * term counts or fewer) runs the unrolled kernel of one of the device's
+ * CDB_MAX_REACTION_TYPES constant-memory slots, which engines and plugin
+ * reactions share (identical parameters and fits share one slot); other fit
+ * sets, or a reaction created when every slot is taken, run the generic
+ * kernel.  Both compute the same model; the slot kernel is faster. */
+
 cdb_status cdb_reaction_create(int device, cdb_precision precision, const cdb_tt06_params* params,
                                const cdb_fit fits[CDB_NUM_FITS], int64_t nCells, double dt,
                                cdb_reaction** out);

@@ -89,3 +89,57 @@ def test_split_plugins_loop_matches_oracle(cdb_lib, oracle_port, fits002):
         time += DT
     sim.step(300)
     assert np.abs(Vm.cpu().numpy() - sim.vm()).max() <= 1e-6
+
+
+def _single_type(n, vm):
+    return tissue.Tissue(n, 1, 1, 1.0, 1.0, 1.0, np.arange(n), np.full(n, 101, np.int32), np.zeros((n, 6)), vm, [])
+
+
+def test_reaction_slots_past_the_last_and_shared(cdb_lib, oracle_port, fits002):
+    """Eight plugin reactions with distinct g_Kr alive at once: the first
+    take constant-memory slots (the compiled per-slot kernel), the rest run
+    the generic kernel; each matches the oracle with its own parameters.
+    A ninth with the first one's content shares its slot."""
+    import dataclasses
+    import torch
+    n = 96
+    rng = np.random.default_rng(1)
+    base = fits002[1]
+    variants = [dataclasses.replace(base, g_Kr=base.g_Kr * (1 + 0.25 * k)) for k in range(8)] + [base]
+    vm0 = -83.0 + rng.uniform(-1, 1, n)
+    vm0[:8] = 20.0      # a few cells depolarised, so g_Kr matters within the run
+    rx = [plugins.BetterTT06(p, n, DT) for p in variants]
+    idx = torch.arange(n, dtype=torch.int32, device="cuda")
+    iStim = torch.zeros(n, dtype=torch.float64, device="cuda")
+    finals = []
+    for r, p in zip(rx, variants):
+        sim = oracle_port.PortSim(_single_type(n, vm0), [p], np.zeros(n, np.uint8), DT, diffusion=False)
+        Vm = torch.from_numpy(vm0.copy()).cuda()
+        dVm = torch.empty_like(Vm)
+        for _ in range(40):
+            r.calc(DT, idx, Vm, iStim, dVm)
+            Vm += DT * dVm
+        sim.step(40)
+        got = Vm.cpu().numpy()
+        assert np.abs(got - sim.vm()).max() <= 1e-9
+        finals.append(got)
+    assert np.abs(finals[0] - finals[1]).max() > 1e-6      # the variants differ
+    np.testing.assert_array_equal(finals[-1], finals[0])   # same content, same slot, same bits
+
+
+def test_engine_shares_slots_with_plugin_reactions(cdb_lib, fits002):
+    """Plugin reactions for the three shipped types hold three slots; an
+    engine registering the same three types shares them, so three more
+    distinct plugin reactions still get slots and the engine still steps."""
+    import dataclasses
+    from cardioid_b200 import engine
+    keep = [plugins.BetterTT06(p, 32, DT) for p in fits002]
+    extra = [plugins.BetterTT06(dataclasses.replace(fits002[0], g_Kr=0.1 * (k + 1)), 32, DT) for k in range(3)]
+    t = tissue.box(12, 10, 8)
+    with engine.Engine(DT, precision="fp64") as e:
+        rx, _ = engine.transmural_setup(e, t, DT)
+        e.add_tissue(t, rx)
+        e.step(20)
+        e.sync()
+        assert np.isfinite(e.read_vm(0)).all()
+    del keep, extra
