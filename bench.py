@@ -115,7 +115,8 @@ def cpu_baseline(steps, warmup, procs=None):
         pass
     what = ("the reference's own CPU path (oracle/_ref: BetterTT06 + FGRDiffusionOMP + BoxStimulus, omp-loop order)"
             if kind == "reference" else "the oracle's C restatement of the reference path")
-    return {"value": cells / wall, "unit": METRIC, "cores": procs, "kind": kind,
+    per_core = sum(r[0] * r[1] / r[2] for r in res) / len(res)
+    return {"value": cells / wall, "unit": METRIC, "cores": procs, "kind": kind, "per_core": per_core,
             "sample": "%s; %d processes (one per host core, like one MPI rank per core, no halo exchange), "
                       "each a %dx%dx%d box of the same workload for %d steps after %d warm-up; CPU: %s"
                       % (what, procs, CPU_SAMPLE[0], CPU_SAMPLE[1], CPU_SAMPLE[2], steps, warmup, cpu)}

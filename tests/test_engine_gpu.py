@@ -314,3 +314,53 @@ def test_staging_modes_agree(cdb_lib, fits002, precision):
         for a, b in zip(out[0], out[stage]):
             for x, y in zip(a, b):
                 np.testing.assert_array_equal(x, y)
+
+
+def _cube_in(n_box, off, side=8, seed=5):
+    """A side^3 cube of tissue (transmural slabs, x = 0 face paced) placed at
+    offset `off` inside an n_box^3 grid (a masked tissue)."""
+    import dataclasses
+    c = tissue.box(side, side, side, dx=0.2, seed=seed)
+    x, y, z = c.tuples()
+    gid = (x + off) + n_box * ((y + off) + n_box * (z + off).astype(np.int64))
+    s = dataclasses.replace(c.stimuli[0], xMin=off - 1, xMax=off + 1, yMin=off - 1, yMax=off + side,
+                            zMin=off - 1, zMax=off + side)
+    return tissue.Tissue(n_box, n_box, n_box, c.dx, c.dy, c.dz, gid.astype(np.int64), c.cell_type, c.sigma, c.vm0,
+                         [s])
+
+
+def test_64bit_voxel_indices_far_corner(cdb_lib, fits002):
+    """The same 8^3 cube in a 10^3 grid and at the far corner of a 1300^3
+    grid (cell gids and padded-voxel indices above 2^31; ~35 GB of padded
+    Vm blocks): bit-identical Vm and activation times after 300 steps."""
+    small = _cube_in(10, 1)
+    big = _cube_in(1300, 1290)
+    assert big.gid.max() > 2 ** 31
+    out = []
+    for t in (small, big):
+        with _engine(fits002) as e:
+            tid = e.add_tissue(t, _reaction_ids(t))
+            e.step(300)
+            e.sync()
+            out.append((e.read_vm(tid), e.read_activation(tid)))
+    np.testing.assert_array_equal(out[0][0], out[1][0])
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    assert (out[0][1] > 0).any()     # the wave started
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (33, 1, 1), (5, 7, 1), (3, 3, 3), (31, 2, 1)])
+def test_tiny_and_ragged_tissues_match_oracle(cdb_lib, oracle_port, fits002, shape):
+    """A single cell, and tissues whose type groups end mid-tile (ragged 32-slot
+    blocks, one-cell groups): FP64 parity with the oracle after 400 steps."""
+    t = tissue.box(*shape, seed=11)
+    rx = _reaction_ids(t)
+    sim = oracle_port.PortSim(t, fits002, rx, DT)
+    sim.step(400)
+    with _engine(fits002) as e:
+        tid = e.add_tissue(t, rx)
+        e.step(400)
+        vm = e.read_vm(tid)
+        act = e.read_activation(tid)
+    assert np.abs(vm - sim.vm()).max() <= VM_TOL_FP64
+    np.testing.assert_array_equal(act, sim.activation())
+    assert (act > 0).any()
