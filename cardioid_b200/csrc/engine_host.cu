@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -84,6 +85,15 @@ struct HostTissue {
   int parity = 0;
   int64_t n = 0;
   int nx = 0, ny = 0, nz = 0;
+  // Chunked host step (cdb_engine_step_host): chunk j holds cells
+  // pipeCell[j] .. pipeCell[j+1]-1, whole planes of the slowest grid axis;
+  // its compute launches take the tiles whose stencil needs no later chunk
+  // (per slot, local tiles up to pipeTiles[j][slot]); its new Vm is final
+  // once compute chunk pipeOut[j] has run.  pipeK = 1: one chunk.
+  int pipeK = 1;
+  std::vector<int64_t> pipeCell;
+  std::vector<int> pipeOut;
+  std::vector<std::array<int64_t, CDB_MAX_REACTION_TYPES>> pipeTiles;
 };
 
 // Constant-memory reaction slots are a per-device resource shared by every
@@ -190,10 +200,37 @@ struct Engine {
     return r > 0 ? r : 4;
   }
 
+  // copy streams and events of the chunked host step
+  cudaStream_t sIn = nullptr, sOut = nullptr;
+  cudaEvent_t evStart = nullptr;
+  std::vector<cudaEvent_t> evIn, evComp;
+  DeviceBuffer dStageOut;
+
+  cudaError_t ensure_pipe(int K)
+  {
+    cudaError_t err = cudaSuccess;
+    if (!sIn) err = cudaStreamCreateWithFlags(&sIn, cudaStreamNonBlocking);
+    if (err == cudaSuccess && !sOut) err = cudaStreamCreateWithFlags(&sOut, cudaStreamNonBlocking);
+    if (err == cudaSuccess && !evStart) err = cudaEventCreateWithFlags(&evStart, cudaEventDisableTiming);
+    while (err == cudaSuccess && (int)evIn.size() < K) {
+      cudaEvent_t a = nullptr, b = nullptr;
+      err = cudaEventCreateWithFlags(&a, cudaEventDisableTiming);
+      if (err == cudaSuccess) err = cudaEventCreateWithFlags(&b, cudaEventDisableTiming);
+      if (a) evIn.push_back(a);
+      if (b) evComp.push_back(b);
+    }
+    return err;
+  }
+
   ~Engine()
   {
     if (graph) cudaGraphExecDestroy(graph);
     tissues.clear();
+    for (cudaEvent_t ev : evIn) cudaEventDestroy(ev);
+    for (cudaEvent_t ev : evComp) cudaEventDestroy(ev);
+    if (evStart) cudaEventDestroy(evStart);
+    if (sIn) cudaStreamDestroy(sIn);
+    if (sOut) cudaStreamDestroy(sOut);
     if (stream) cudaStreamDestroy(stream);
     for (int t = 0; t < nTypes; ++t) release_slot(cfg.device, slots[t]);
   }
@@ -307,6 +344,30 @@ struct Engine {
     return nullptr;
   }
 
+  // Step s of a batch for tiles first .. first+count-1 of the table (all
+  // of slot rt).
+  void launch_tiles(int rt, int64_t first, int64_t count, int s, bool minmax, cudaStream_t st)
+  {
+    StepArgs a;
+    a.tissues = dTissues.as<TissueDev>();
+    a.tiles = dTiles.as<WarpTile>() + first;
+    a.nTiles = (int)count;
+    a.rt = rt;
+    a.stims = dStims.as<cdb_stimulus>();
+    a.times = dTimes.as<double>();
+    a.dt = cfg.dt;
+    a.k = s;
+    a.minmax = minmax ? 1 : 0;
+    a.stage = stage;
+    a.err = dErr.as<int>();
+    const int slot = spec[rt] ? rt : -1;
+    const unsigned grid = (unsigned)std::min<int64_t>(grid_for(a.nTiles, kWarpsPerCta),
+                                                      (int64_t)numSms * grid_ctas_per_sm(slot));
+    if (cfg.precision == CDB_MIXED) launch_step<true>(slot, anyEcg, grid, st, a);
+    else launch_step<false>(slot, anyEcg, grid, st, a);
+    ++launches;
+  }
+
   cdb_status launch_batch(int k, bool minmax)
   {
     const int nT = (int)order.size();
@@ -314,28 +375,9 @@ struct Engine {
       reset_minmax_kernel<<<grid_for(nT, 128), 128, 0, stream>>>(dTissues.as<TissueDev>(), nT);
       ++launches;
     }
-    for (int s = 0; s < k; ++s) {
-      for (const auto& st : slotTiles) {
-        StepArgs a;
-        a.tissues = dTissues.as<TissueDev>();
-        a.tiles = dTiles.as<WarpTile>() + st.second.first;
-        a.nTiles = st.second.second;
-        a.rt = st.first;
-        a.stims = dStims.as<cdb_stimulus>();
-        a.times = dTimes.as<double>();
-        a.dt = cfg.dt;
-        a.k = s;
-        a.minmax = (minmax && s == k - 1) ? 1 : 0;
-        a.stage = stage;
-        a.err = dErr.as<int>();
-        const int slot = spec[st.first] ? st.first : -1;
-        const unsigned grid = (unsigned)std::min<int64_t>(grid_for(a.nTiles, kWarpsPerCta),
-                                                          (int64_t)numSms * grid_ctas_per_sm(slot));
-        if (cfg.precision == CDB_MIXED) launch_step<true>(slot, anyEcg, grid, stream, a);
-        else launch_step<false>(slot, anyEcg, grid, stream, a);
-        ++launches;
-      }
-    }
+    for (int s = 0; s < k; ++s)
+      for (const auto& st : slotTiles)
+        launch_tiles(st.first, st.second.first, st.second.second, s, minmax && s == k - 1, stream);
     advance_kernel<<<grid_for(nT, 128), 128, 0, stream>>>(dTissues.as<TissueDev>(), nT, k);
     ++launches;
     return CDB_OK;
@@ -526,6 +568,77 @@ int64_t count_slots(int64_t n, const uint8_t* reaction, const int* slots, int64_
 // group starting on a 32-slot block, so every AoSoA block holds one type and
 // every warp tile is full but the last of its type (the per-type cell
 // grouping of ReactionManager::create, elec/ReactionManager.cc:74-371).
+// The chunk plan of cdb_engine_step_host.  Cells must be in grid order
+// (non-decreasing gid), so a chunk of whole planes of the slowest axis is a
+// range of cells and every reaction type's tiles reach those planes in
+// order; a tile needs the planes of its cells and one past them (the
+// stencil), so it is computed by the chunk holding its last cell's next
+// plane.  One chunk when the tissue is small or out of grid order.
+void build_pipe(HostTissue& h, const int64_t* gid, const std::vector<int64_t>& cellOf)
+{
+  h.pipeK = 1;
+  h.pipeCell = {0, h.n};
+  h.pipeOut = {0};
+  h.pipeTiles.assign(1, {});
+  for (int k = 0; k < CDB_MAX_REACTION_TYPES; ++k) h.pipeTiles[0][k] = (int64_t)h.tiles[k].size();
+  const int64_t n = h.n;
+  int64_t stride = 1, planes = h.nx;
+  if (h.nz > 1) {
+    stride = (int64_t)h.nx * h.ny;
+    planes = h.nz;
+  } else if (h.ny > 1) {
+    stride = h.nx;
+    planes = h.ny;
+  }
+  // 16 chunks measured best on the 256^3 box (3.4 ms per step against 3.8
+  // with 8 and 3.7 with 32: more chunks shorten the pipeline's tail, fewer
+  // keep the step launches long)
+  const int K = (int)std::min<int64_t>(16, planes / 16);
+  if (K < 2 || n < (int64_t(1) << 16)) return;
+  auto g = [&](int64_t c) { return gid ? gid[c] : c; };
+  for (int64_t c = 1; c < n; ++c)
+    if (g(c) < g(c - 1)) return;
+  auto plane = [&](int64_t c) { return g(c) / stride; };
+  std::vector<int64_t> P(K + 1);   // chunk j: planes P[j] .. P[j+1]-1
+  for (int j = 0; j <= K; ++j) P[j] = j * planes / K;
+  auto chunk_of = [&](int64_t p) {
+    int j = 0;
+    while (j + 1 < K && P[j + 1] <= p) ++j;
+    return j;
+  };
+  std::vector<int64_t> cells(K + 1, n);
+  for (int j = 0; j < K; ++j) {
+    int64_t lo = 0, hi = n;   // first cell with plane >= P[j]
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) / 2;
+      if (plane(mid) >= P[j]) hi = mid;
+      else lo = mid + 1;
+    }
+    cells[j] = lo;
+  }
+  cells[0] = 0;
+  std::vector<int> out(K, 0);
+  std::vector<std::array<int64_t, CDB_MAX_REACTION_TYPES>> ends(K);
+  for (int k = 0; k < CDB_MAX_REACTION_TYPES; ++k) {
+    std::vector<int64_t> count(K, 0);
+    int prev = 0;
+    for (const WarpTile& tl : h.tiles[k]) {
+      const int64_t c0 = cellOf[tl.first], c1 = cellOf[tl.first + tl.count - 1];
+      const int req = chunk_of(std::min<int64_t>(plane(c1) + 1, planes - 1));
+      if (req < prev) return;
+      prev = req;
+      ++count[req];
+      for (int ch = chunk_of(plane(c0)); ch <= chunk_of(plane(c1)); ++ch) out[ch] = std::max(out[ch], req);
+    }
+    int64_t acc = 0;
+    for (int j = 0; j < K; ++j) ends[j][k] = acc += count[j];
+  }
+  h.pipeK = K;
+  h.pipeCell = std::move(cells);
+  h.pipeOut = std::move(out);
+  h.pipeTiles = std::move(ends);
+}
+
 // Fills h.slot, h.tiles, h.nSlots and vrel (per slot: voxel offset from its
 // tile's first voxel; 0 for padding).
 cdb_status build_layout(HostTissue& h, const int64_t* gid, const uint8_t* reaction, const int* slots,
@@ -541,11 +654,12 @@ cdb_status build_layout(HostTissue& h, const int64_t* gid, const uint8_t* reacti
     total += (count[k] + kBlk - 1) / kBlk * kBlk;
   }
   h.slot.resize(n);
-  std::vector<int64_t> voxOf(h.nSlots, 0);
+  std::vector<int64_t> voxOf(h.nSlots, 0), cellOf(h.nSlots, -1);
   std::vector<unsigned> mask(h.nSlots / kBlk, 0u);
   for (int64_t c = 0; c < n; ++c) {
     const int64_t i = next[slots[reaction[c]]]++;
     h.slot[c] = i;
+    cellOf[i] = c;
     const int64_t g = gid ? gid[c] : c;
     const int x = (int)(g % h.nx);
     const int64_t yz = g / h.nx;
@@ -573,6 +687,7 @@ cdb_status build_layout(HostTissue& h, const int64_t* gid, const uint8_t* reacti
       }
       h.tiles[k].push_back(tl);
     }
+  build_pipe(h, gid, cellOf);
   return CDB_OK;
 }
 
@@ -825,7 +940,7 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
       fill_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, v0.as<double>(), kInitialVm);
       E.launches += 1;
     }
-    scatter_vm_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, v0.as<double>(), d.vm[0], d.voxel, d.nx, d.ny, d.px,
+    scatter_vm_kernel<<<grid_for(n, 256), 256, 0, s>>>(0, n, v0.as<double>(), d.vm[0], d.voxel, d.nx, d.ny, d.px,
                                                        d.pxy, d.py0, d.pz0, nullptr);
     E.launches += 1;
     CDB_CUDA(cudaStreamSynchronize(s));
@@ -986,7 +1101,7 @@ cdb_status cdb_engine_read_vm(cdb_engine* e, int32_t id, double* host)
   DeviceBuffer tmp;
   CDB_CUDA(tmp.alloc(t->n * 8));
   const TissueDev& d = t->dev;
-  gather_vm_kernel<<<grid_for(t->n, 256), 256, 0, E.stream>>>(t->n, d.vm[t->parity], tmp.as<double>(), d.voxel,
+  gather_vm_kernel<<<grid_for(t->n, 256), 256, 0, E.stream>>>(0, t->n, d.vm[t->parity], tmp.as<double>(), d.voxel,
                                                              d.nx, d.ny, d.px, d.pxy, d.py0, d.pz0);
   E.launches += 1;
   CDB_CUDA(cudaMemcpyAsync(host, tmp.p, t->n * 8, cudaMemcpyDeviceToHost, E.stream));
@@ -1006,7 +1121,7 @@ cdb_status cdb_engine_write_vm(cdb_engine* e, int32_t id, const double* host)
   CDB_CUDA(cudaMemcpyAsync(tmp.p, host, t->n * 8, cudaMemcpyHostToDevice, E.stream));
   const TissueDev& d = t->dev;
   t->dev.actAll = 1;
-  scatter_vm_kernel<<<grid_for(t->n, 256), 256, 0, E.stream>>>(t->n, tmp.as<double>(), d.vm[t->parity], d.voxel,
+  scatter_vm_kernel<<<grid_for(t->n, 256), 256, 0, E.stream>>>(0, t->n, tmp.as<double>(), d.vm[t->parity], d.voxel,
                                                               d.nx, d.ny, d.px, d.pxy, d.py0, d.pz0,
                                                               E.act_all_flag(id));
   E.launches += 1;
@@ -1132,19 +1247,84 @@ cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, 
   CDB_CUDA(cudaSetDevice(E.cfg.device));
   const int64_t n = t->n;
   if (E.dStage.bytes < (size_t)n * 8) CDB_CUDA(E.dStage.alloc(n * 8));
-  const TissueDev& d = t->dev;
   cudaStream_t s = E.stream;
-  CDB_CUDA(cudaMemcpyAsync(E.dStage.p, vm_in, n * 8, cudaMemcpyHostToDevice, s));
-  t->dev.actAll = 1;
-  scatter_vm_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, E.dStage.as<double>(), d.vm[t->parity], d.voxel, d.nx, d.ny,
-                                                     d.px, d.pxy, d.py0, d.pz0, E.act_all_flag(id));
-  E.launches += 1;
-  cdb_status st = E.step(1, false);
+  if (t->pipeK < 2) {
+    const TissueDev& d = t->dev;
+    CDB_CUDA(cudaMemcpyAsync(E.dStage.p, vm_in, n * 8, cudaMemcpyHostToDevice, s));
+    t->dev.actAll = 1;
+    scatter_vm_kernel<<<grid_for(n, 256), 256, 0, s>>>(0, n, E.dStage.as<double>(), d.vm[t->parity], d.voxel, d.nx,
+                                                       d.ny, d.px, d.pxy, d.py0, d.pz0, E.act_all_flag(id));
+    E.launches += 1;
+    cdb_status st = E.step(1, false);
+    if (st != CDB_OK) return st;
+    gather_vm_kernel<<<grid_for(n, 256), 256, 0, s>>>(0, n, d.vm[t->parity], E.dStage.as<double>(), d.voxel, d.nx,
+                                                      d.ny, d.px, d.pxy, d.py0, d.pz0);
+    E.launches += 1;
+    CDB_CUDA(cudaMemcpyAsync(vm_out, E.dStage.p, n * 8, cudaMemcpyDeviceToHost, s));
+    CDB_CUDA(cudaStreamSynchronize(s));
+    return CDB_OK;
+  }
+  // Chunked: Vm goes up chunk by chunk on one copy stream; on the engine's
+  // stream each chunk is scattered into the padded block once it has
+  // landed, the tiles whose stencil reads no later chunk are computed, and
+  // the chunks whose new Vm is then final are gathered; a second copy
+  // stream takes each of those down.  Both copy directions and the step
+  // overlap, and every kernel stays on the engine's stream (the persistent
+  // step kernels hold every SM while they run).
+  cdb_status st = E.ensure_times(1);
   if (st != CDB_OK) return st;
-  gather_vm_kernel<<<grid_for(n, 256), 256, 0, s>>>(n, d.vm[t->parity], E.dStage.as<double>(), d.voxel, d.nx, d.ny,
-                                                    d.px, d.pxy, d.py0, d.pz0);
+  st = E.rebuild();
+  if (st != CDB_OK) return st;
+  const int K = t->pipeK;
+  CDB_CUDA(E.ensure_pipe(K));
+  if (E.dStageOut.bytes < (size_t)n * 8) CDB_CUDA(E.dStageOut.alloc(n * 8));
+  const TissueDev& d = t->dev;
+  double* const vin = d.vm[t->parity];
+  double* const vout = d.vm[t->parity ^ 1];
+  int* const flag = E.act_all_flag(id);
+  t->dev.actAll = 1;
+  double* const stIn = E.dStage.as<double>();
+  double* const stOut = E.dStageOut.as<double>();
+  CDB_CUDA(cudaEventRecord(E.evStart, s));
+  CDB_CUDA(cudaStreamWaitEvent(E.sIn, E.evStart, 0));
+  CDB_CUDA(cudaStreamWaitEvent(E.sOut, E.evStart, 0));
+  for (int j = 0; j < K; ++j) {
+    const int64_t c0 = t->pipeCell[j], m = t->pipeCell[j + 1] - c0;
+    if (m > 0) CDB_CUDA(cudaMemcpyAsync(stIn + c0, vm_in + c0, m * 8, cudaMemcpyHostToDevice, E.sIn));
+    CDB_CUDA(cudaEventRecord(E.evIn[j], E.sIn));
+  }
+  for (int j = 0; j < K; ++j) {
+    CDB_CUDA(cudaStreamWaitEvent(s, E.evIn[j], 0));
+    const int64_t c0 = t->pipeCell[j], m = t->pipeCell[j + 1] - c0;
+    if (m > 0) {
+      scatter_vm_kernel<<<grid_for(m, 256), 256, 0, s>>>(c0, m, stIn, vin, d.voxel, d.nx, d.ny, d.px, d.pxy, d.py0,
+                                                         d.pz0, flag);
+      E.launches += 1;
+    }
+    for (const auto& sl : E.slotTiles) {
+      const int64_t lo = j ? t->pipeTiles[j - 1][sl.first] : 0, hi = t->pipeTiles[j][sl.first];
+      if (hi > lo) E.launch_tiles(sl.first, sl.second.first + lo, hi - lo, 0, false, s);
+    }
+    for (int i = 0; i < K; ++i) {
+      const int64_t g0 = t->pipeCell[i], gm = t->pipeCell[i + 1] - g0;
+      if (t->pipeOut[i] != j || gm == 0) continue;
+      gather_vm_kernel<<<grid_for(gm, 256), 256, 0, s>>>(g0, gm, vout, stOut, d.voxel, d.nx, d.ny, d.px, d.pxy, d.py0,
+                                                         d.pz0);
+      E.launches += 1;
+    }
+    CDB_CUDA(cudaEventRecord(E.evComp[j], s));
+  }
+  advance_kernel<<<1, 128, 0, s>>>(E.dTissues.as<TissueDev>(), 1, 1);
   E.launches += 1;
-  CDB_CUDA(cudaMemcpyAsync(vm_out, E.dStage.p, n * 8, cudaMemcpyDeviceToHost, s));
+  E.advance_host(1);
+  for (int j = 0; j < K; ++j) {
+    const int64_t c0 = t->pipeCell[j], m = t->pipeCell[j + 1] - c0;
+    if (m == 0) continue;
+    CDB_CUDA(cudaStreamWaitEvent(E.sOut, E.evComp[t->pipeOut[j]], 0));
+    CDB_CUDA(cudaMemcpyAsync(vm_out + c0, stOut + c0, m * 8, cudaMemcpyDeviceToHost, E.sOut));
+  }
+  CDB_CUDA(cudaGetLastError());
+  CDB_CUDA(cudaStreamSynchronize(E.sOut));
   CDB_CUDA(cudaStreamSynchronize(s));
   return CDB_OK;
 }

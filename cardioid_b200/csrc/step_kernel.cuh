@@ -740,23 +740,25 @@ __device__ __forceinline__ int64_t cell_voxel(int64_t i, const int64_t* __restri
   return (x + 1) + px * (y + py0) + pxy * (z + pz0);
 }
 
-// Writes host-given Vm into a padded block; sets *actAll (when given) so the
-// next step checks every cell's activation time.
-__global__ void scatter_vm_kernel(int64_t n, const double* __restrict__ src, double* __restrict__ blk,
+// Writes host-given Vm of cells c0 .. c0+n-1 into a padded block; sets
+// *actAll (when given) so the next step checks every cell's activation time.
+__global__ void scatter_vm_kernel(int64_t c0, int64_t n, const double* __restrict__ src, double* __restrict__ blk,
                                   const int64_t* __restrict__ voxel, int nx, int ny, int64_t px, int64_t pxy, int py0,
                                   int pz0, int* actAll)
 {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) blk[cell_voxel(i, voxel, nx, ny, px, pxy, py0, pz0)] = src[i];
-  if (i == 0 && actAll) *actAll = 1;
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t i = c0 + j;
+  if (j < n) blk[cell_voxel(i, voxel, nx, ny, px, pxy, py0, pz0)] = src[i];
+  if (j == 0 && actAll) *actAll = 1;
 }
 
-__global__ void gather_vm_kernel(int64_t n, const double* __restrict__ blk, double* __restrict__ dst,
+__global__ void gather_vm_kernel(int64_t c0, int64_t n, const double* __restrict__ blk, double* __restrict__ dst,
                                  const int64_t* __restrict__ voxel, int nx, int ny, int64_t px, int64_t pxy, int py0,
                                  int pz0)
 {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i < n) dst[i] = blk[cell_voxel(i, voxel, nx, ny, px, pxy, py0, pz0)];
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t i = c0 + j;
+  if (j < n) dst[i] = blk[cell_voxel(i, voxel, nx, ny, px, pxy, py0, pz0)];
 }
 
 // Row var of the AoSoA state to / from a cell-order array of doubles

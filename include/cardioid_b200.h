@@ -263,7 +263,12 @@ cdb_status cdb_engine_read_weights(cdb_engine* e, int32_t id, double* host19);
  * one fused step of the tissue and copies the new Vm to vm_out (host).
  * The reaction state stays on the device, as a Reaction object keeps its
  * own state; this is the per-step cost a caller that owns Vm on the host
- * pays. */
+ * pays.  The engine must hold only this tissue.  When its cells are in grid
+ * order (non-decreasing gid) and it has at least 32 planes along its
+ * slowest axis and 65536 cells, the step runs in chunks of planes so the
+ * upload, the step and the download overlap (both copy directions need
+ * page-locked host buffers to overlap); vm_in and vm_out may be the same
+ * buffer. */
 cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, double* vm_out);
 /* ------------------------------------------------------------------ */
 /* Diagnostics                                                           */

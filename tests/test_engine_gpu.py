@@ -165,6 +165,35 @@ def test_step_host_equals_device_step(cdb_lib, fits002):
         np.testing.assert_array_equal(vm, ref)
 
 
+@pytest.mark.parametrize("kind,precision", [("box", "fp64"), ("box", "mixed"), ("sheet", "mixed"),
+                                            ("masked", "fp64")])
+def test_chunked_step_host_equals_device_steps(cdb_lib, fits002, kind, precision):
+    """cdb_engine_step_host on tissues large enough for its chunked pipeline
+    (64^3 box: 4 chunks of z-planes; a 512 x 256 sheet: 8 chunks of rows; a
+    masked box: 2 chunks): Vm, activation times and states bit-identical to
+    device-resident steps, across the stimulus and the wave it starts."""
+    t = {"box": lambda: tissue.box(64, 64, 64), "sheet": lambda: tissue.box(512, 256, 1),
+         "masked": lambda: _masked(64, 48, 40)}[kind]()
+    steps = 120
+    with _engine(fits002, precision) as e:
+        tid = e.add_tissue(t, _reaction_ids(t))
+        e.step(steps)
+        ref = (e.read_vm(tid), e.read_activation(tid), e.read_states(tid))
+    with _engine(fits002, precision) as e:
+        tid = e.add_tissue(t, _reaction_ids(t))
+        vm = np.ascontiguousarray(t.vm0, dtype=np.float64)
+        out = np.empty_like(vm)
+        for _ in range(steps):
+            e.step_host(tid, vm, out)
+            vm, out = out, vm
+        np.testing.assert_array_equal(vm, ref[0])
+        np.testing.assert_array_equal(e.read_vm(tid), ref[0])
+        np.testing.assert_array_equal(e.read_activation(tid), ref[1])
+        np.testing.assert_array_equal(e.read_states(tid), ref[2])
+        assert e.time(tid)[0] == steps
+    assert (ref[1] > 0).any()
+
+
 @pytest.mark.parametrize("graphs", [True, False])
 def test_activation_after_host_vm_writes(cdb_lib, oracle_port, fits002, graphs):
     """The engine reads a cell's activation time only on upward crossings of
