@@ -3,7 +3,8 @@ stepped together by one engine — continuous batching.  Between launch
 batches the loop admits waiting jobs first come, first served while the
 device has memory for them (cdb_engine_tissue_bytes against free memory),
 steps every active job, and retires the finished ones, reading back their
-activation maps.  Reports time-to-result percentiles and the aggregate
+activation maps.  Worker threads build arrived jobs' tissues on the host
+meanwhile, so a large job's set-up does not stall the active ones.  Reports time-to-result percentiles and the aggregate
 cell-steps/s.
 
 The engine runs each tissue on its own clock and step count, so a job's
@@ -15,6 +16,7 @@ On N GPUs, one process per GPU serves its own share of the jobs
 import collections
 import math
 import time
+from concurrent.futures import Future, ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -111,10 +113,12 @@ class Server:
                its end, so it is cut to the fewest steps any job has left
     reserve    device bytes kept free beyond each admitted tissue
     keep       keep each job's activation map in its result
+    workers    threads that build arrived jobs' tissues on the host while
+               the device steps the active ones (0: build at admission)
     """
 
     def __init__(self, engine, reactions, batch=200, reserve=1 << 30, keep=False, clock=time.perf_counter,
-                 sleep=time.sleep, build=pop.build):
+                 sleep=time.sleep, build=pop.build, workers=2):
         self.engine = engine
         self.reactions = list(reactions)
         self.batch = int(batch)
@@ -123,16 +127,29 @@ class Server:
         self.clock = clock
         self.sleep = sleep
         self.build = build
+        self.workers = int(workers)
         self.cell_steps = 0
         self.rejected = []
         self._built = {}
+        self._pool = None
+
+    def _arrived(self, job):
+        if self._pool is not None:
+            self._built[job.id] = self._pool.submit(self.build, job.instance)
 
     def _admit(self, job, now, alone):
-        """(tissue id, state) once admitted, None to wait for memory, or
-        "reject" when the job cannot fit even alone."""
+        """(tissue id, state) once admitted, None to wait (for memory, or for
+        the job's tissue to be built), or "reject" when the job cannot fit
+        even alone."""
         inst = job.instance
-        if job.id not in self._built:
-            t = self.build(inst)
+        entry = self._built.get(job.id)
+        if entry is None or isinstance(entry, Future):
+            if entry is None:
+                t = self.build(inst)
+            elif not entry.done():
+                return None
+            else:
+                t = entry.result()
             rx = np.full(t.n, self.reactions[inst.celltype], np.uint8)
             self._built[job.id] = (t, rx, self.engine.tissue_bytes(t, rx, inst.scales))
         t, rx, need = self._built[job.id]
@@ -150,13 +167,25 @@ class Server:
         waiting = collections.deque()
         active = {}
         results = []
+        if self.workers > 0:
+            self._pool = ThreadPoolExecutor(max_workers=self.workers)
+        try:
+            return self._serve(pending, waiting, active, results, max_seconds)
+        finally:
+            if self._pool is not None:
+                self._pool.shutdown(wait=True, cancel_futures=True)
+                self._pool = None
+
+    def _serve(self, pending, waiting, active, results, max_seconds):
         t0 = self.clock()
         while pending or waiting or active:
             now = self.clock() - t0
             if max_seconds is not None and now > max_seconds:
                 break
             while pending and pending[0].arrival <= now:
-                waiting.append(pending.popleft())
+                job = pending.popleft()
+                waiting.append(job)
+                self._arrived(job)
             while waiting:
                 got = self._admit(waiting[0], now, alone=not active)
                 if got is None:
@@ -169,7 +198,9 @@ class Server:
                 tid, state = got
                 active[tid] = state
             if not active:
-                if pending:
+                if waiting:
+                    self.sleep(0.001)      # the head of the queue is being built
+                elif pending:
                     self.sleep(max(0.0, min(0.01, pending[0].arrival - (self.clock() - t0))))
                 continue
             k = min(self.batch, min(s["left"] for s in active.values()))

@@ -186,3 +186,18 @@ def test_served_job_equals_job_alone(cdb_lib, fits002):
             tid = e.add_tissue(t, np.full(t.n, rid[inst.celltype], np.uint8), scales=inst.scales)
             e.step(700)
             np.testing.assert_array_equal(e.read_activation(tid), r.activation)
+
+
+def test_server_builds_on_worker_threads_with_the_same_results():
+    """Tissues built on worker threads (the default) or at admission serve
+    the same jobs to the same results, first come first served."""
+    jobs = _jobs(n=30, seed=7)
+    out = {}
+    for workers in (0, 2):
+        eng = FakeEngine(total=100 * 120000)
+        srv = _server(eng, batch=97, keep=True, workers=workers)
+        res = srv.run(jobs)
+        assert [i for op, i in eng.log] == sorted(i for op, i in eng.log)
+        out[workers] = sorted((r.id, r.cells, r.steps, r.activated, tuple(r.activation)) for r in res)
+    assert out[0] == out[2]
+    assert [r[0] for r in out[0]] == [j.id for j in jobs]
