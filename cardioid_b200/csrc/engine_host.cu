@@ -78,6 +78,7 @@ struct HostTissue {
   std::vector<int64_t> slot;        // slot of every cell
   DeviceBuffer slotMap, vrel;       // device copies: cell -> slot; per-slot voxel offsets
   DeviceBuffer ecgPts, ecgTrace;    // ECG electrodes and trace ring (cdb_engine_set_ecg)
+  DeviceBuffer ecgInvr;             // 1/r per slot and electrode
   double ecgK = 0;                  // kconst * dx dy dz
   int64_t ecgNext = 0;              // next evaluation (step / rate) to hand to the host
   int64_t steps = 0;       // steps taken
@@ -1016,9 +1017,22 @@ cdb_status cdb_engine_set_ecg(cdb_engine* e, int32_t id, int32_t nPoints, const 
     d.ecgN = 0;
     t->ecgPts.release();
     t->ecgTrace.release();
+    t->ecgInvr.release();
   } else {
     CDB_CUDA(t->ecgPts.alloc(nPoints * 3 * sizeof(double)));
     CDB_CUDA(cudaMemcpy(t->ecgPts.p, xyz, nPoints * 3 * sizeof(double), cudaMemcpyHostToDevice));
+    const bool mixed = E.cfg.precision == CDB_MIXED;
+    const size_t invrBytes = (size_t)t->nSlots * nPoints * (mixed ? sizeof(float) : sizeof(double));
+    CDB_CUDA(t->ecgInvr.alloc(invrBytes));
+    CDB_CUDA(cudaMemset(t->ecgInvr.p, 0, invrBytes));
+    if (t->n > 0) {
+      ecg_invr_kernel<<<grid_for(t->n, 256), 256, 0, E.stream>>>(
+          t->n, t->slotMap.as<int64_t>(), d.voxel, d.nx, d.ny, d.px, d.pxy, d.py0, d.pz0, d.hx, d.hy, d.hz,
+          t->ecgPts.as<double>(), nPoints, mixed ? 1 : 0, t->ecgInvr.p);
+      E.launches += 1;
+      CDB_CUDA(cudaGetLastError());
+      CDB_CUDA(cudaStreamSynchronize(E.stream));
+    }
     CDB_CUDA(t->ecgTrace.alloc((size_t)kEcgRing * nPoints * sizeof(double)));
     CDB_CUDA(cudaMemset(t->ecgTrace.p, 0, (size_t)kEcgRing * nPoints * sizeof(double)));
     d.ecgN = nPoints;
@@ -1028,6 +1042,7 @@ cdb_status cdb_engine_set_ecg(cdb_engine* e, int32_t id, int32_t nPoints, const 
   }
   d.ecgPts = t->ecgPts.as<double>();
   d.ecgTrace = t->ecgTrace.as<double>();
+  d.ecgInvr = t->ecgInvr.p;
   E.dirty = true;
   return CDB_OK;
 }

@@ -57,10 +57,14 @@ struct TissueDev {
   unsigned long long* minmax;   // 2 slots
   // ECG pseudo-sensor (off when ecgN == 0): electrodes at ecgPts (x y z, mm),
   // evaluated when the step count reaches a multiple of ecgRate into entry
-  // (count / ecgRate) % kEcgRing of ecgTrace ([kEcgRing][ecgN]).
+  // (count / ecgRate) % kEcgRing of ecgTrace ([kEcgRing][ecgN]); ecgInvr
+  // holds 1 / |r - p_j| per slot ([block][electrode][32], double on the
+  // FP64 path, float on the mixed path; the reference's 1/r table,
+  // elec/ECGSensor.cu:9-40).
   int ecgN, ecgRate;
   const double* ecgPts;
   double* ecgTrace;
+  const void* ecgInvr;
   double hx, hy, hz;          // voxel spacing, mm
 };
 
@@ -90,12 +94,15 @@ struct MinMaxAcc {
   int tissue;
 };
 
-// A warp's running ECG sum (lane j: electrode j) for one tissue and one
-// evaluation entry, added to the trace when either changes.
+// A warp's running ECG sums for one tissue and one evaluation entry, in
+// shared memory (acc[j]: electrode j), added to the trace when either
+// changes.
 struct EcgAcc {
-  double v;
+  double* acc;
   int tissue;
   int entry;
+  int seen = -1;        // tissue whose evaluation entry is evalEntry (-1: none this launch)
+  int evalEntry = -1;
 };
 
 struct StepArgs {
@@ -269,12 +276,33 @@ __device__ __forceinline__ void minmax_flush(const StepArgs& a, MinMaxAcc& acc, 
 
 __device__ __forceinline__ void ecg_flush(const StepArgs& a, EcgAcc& acc, int lane)
 {
+  __syncwarp();
   if (acc.tissue >= 0) {
     const TissueDev* __restrict__ T = a.tissues + acc.tissue;
-    if (lane < T->ecgN) atomicAdd(T->ecgTrace + (int64_t)acc.entry * T->ecgN + lane, acc.v);
+    if (lane < T->ecgN) atomicAdd(T->ecgTrace + (int64_t)acc.entry * T->ecgN + lane, acc.acc[lane]);
   }
+  acc.acc[lane] = 0.0;
+  __syncwarp();
   acc.tissue = -1;
-  acc.v = 0.0;
+}
+
+// Sums 8 values per lane over the warp with 9 shuffles (instead of 8 x 5):
+// each round halves the values a lane keeps and swaps the other half with
+// the partner lane.  Lane l ends with the sum of value (l >> 2) & 7.
+__device__ __forceinline__ double warp_sum8(const double (&v)[8], int lane)
+{
+  const bool h4 = lane & 16, h3 = lane & 8, h2 = lane & 4;
+  double w[4], u[2];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    w[q] = (h4 ? v[q + 4] : v[q]) + __shfl_xor_sync(0xffffffffu, h4 ? v[q] : v[q + 4], 16);
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+    u[q] = (h3 ? w[q + 2] : w[q]) + __shfl_xor_sync(0xffffffffu, h3 ? w[q] : w[q + 2], 8);
+  double r = (h2 ? u[1] : u[0]) + __shfl_xor_sync(0xffffffffu, h2 ? u[0] : u[1], 4);
+  r += __shfl_xor_sync(0xffffffffu, r, 2);
+  r += __shfl_xor_sync(0xffffffffu, r, 1);
+  return r;
 }
 
 // ---- bulk (TMA) staging: one lane issues cp.async.bulk copies of the
@@ -479,24 +507,32 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
   // ECG (ECGSensor::eval / calcEcg, elec/ECGSensor.cc:231-320 and
   // elec/ECGSensor.cu:9-168): after the step, on evaluation steps, electrode
   // j gets sum over cells of dVmD / |r - p_j| with r = (x dx, y dy, z dz).
-  const int ecgN = ECG ? Tp->ecgN : 0;
-  if (ECG && ecgN && (lstep + 1) % Tp->ecgRate == 0) {
-    const int entry = (int)(((lstep + 1) / Tp->ecgRate) % kEcgRing);
+  // Whether this launch evaluates a tissue is fixed per tissue: the warp
+  // works it out when its tiles move to another tissue.
+  if (ECG && ecg.seen != tile.tissue) {
+    ecg.seen = tile.tissue;
+    ecg.evalEntry = Tp->ecgN && (lstep + 1) % Tp->ecgRate == 0 ? (int)(((lstep + 1) / Tp->ecgRate) % kEcgRing) : -1;
+  }
+  if (ECG && ecg.evalEntry >= 0) {
+    const int ecgN = Tp->ecgN;
+    const int entry = ecg.evalEntry;
     if (ecg.tissue != tile.tissue || ecg.entry != entry) {
       ecg_flush(a, ecg, lane);
       ecg.tissue = tile.tissue;
       ecg.entry = entry;
     }
-    const int64_t zz = vox / pxy, rem = vox - zz * pxy, yy = rem / px;
-    const double xr = (double)((int)(rem - yy * px) - 1) * Tp->hx;
-    const double yr = (double)((int)yy - Tp->py0) * Tp->hy;
-    const double zr = (double)((int)zz - Tp->pz0) * Tp->hz;
-    for (int j = 0; j < ecgN; ++j) {
-      const double* p = Tp->ecgPts + 3 * j;
-      const double ex = xr - p[0], ey = yr - p[1], ez = zr - p[2];
-      double c = active ? ecgSrc * (1.0 / sqrt(ex * ex + ey * ey + ez * ez)) : 0.0;
-      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-      if (lane == j) ecg.v += c;
+    const int64_t b = i / kBlk, at = b * ecgN * kBlk + (i - b * kBlk);
+    const double* __restrict__ inv64 = (const double*)Tp->ecgInvr + at;
+    const float* __restrict__ inv32 = (const float*)Tp->ecgInvr + at;
+    for (int g = 0; g < ecgN; g += 8) {
+      double v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        v[q] = active && g + q < ecgN ? ecgSrc * (MIXED ? (double)inv32[(g + q) * kBlk] : inv64[(g + q) * kBlk])
+                                      : 0.0;
+      const double sum = warp_sum8(v, lane);
+      const int e = g + ((lane >> 2) & 7);
+      if ((lane & 3) == 0 && e < ecgN) ecg.acc[e] += sum;
     }
     // the tissue's first tile clears the entry the next evaluation fills
     if (tile.first == 0 && lane < ecgN)
@@ -525,15 +561,21 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
 {
   constexpr int kBuf = stage_bytes<MIXED>();
   __shared__ __align__(16) unsigned char smem[kWarpsPerCta * 2 * kBuf + kWarpsPerCta * 2 * 8];
+  __shared__ double ecgSmem[ECG ? kWarpsPerCta * 32 : 1];   // each warp's ECG sums
   const int lane = threadIdx.x & 31;
   const int warpInCta = threadIdx.x >> 5;
+  double* const ecgMine = ecgSmem + (ECG ? warpInCta * 32 : 0);
+  if (ECG) {
+    ecgMine[lane] = 0.0;
+    __syncwarp();
+  }
   unsigned char* mine = smem + warpInCta * 2 * kBuf;
   const int stride = gridDim.x * kWarpsPerCta;
   int t = blockIdx.x * kWarpsPerCta + warpInCta;
   if (!a.stage) {
     // the next tile's descriptor is in flight while this tile computes
     WarpTile cur, nxt;
-    EcgAcc ecg{0.0, -1, 0};
+    EcgAcc ecg{ecgMine, -1, 0};
     MinMaxAcc mm{__longlong_as_double(0x7ff0000000000000ll), -__longlong_as_double(0x7ff0000000000000ll), -1};
     if (t < a.nTiles) cur = a.tiles[t];
     for (; t < a.nTiles; t += stride) {
@@ -559,7 +601,7 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
-    EcgAcc ecg{0.0, -1, 0};
+    EcgAcc ecg{ecgMine, -1, 0};
     MinMaxAcc mm{__longlong_as_double(0x7ff0000000000000ll), -__longlong_as_double(0x7ff0000000000000ll), -1};
     WarpTile cur = t < a.nTiles ? a.tiles[t] : WarpTile{};
     if (t < a.nTiles && lane == 0)
@@ -596,7 +638,7 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
   }
   cp_async_commit();
   WarpTile cur = t < a.nTiles ? a.tiles[t] : WarpTile{};
-  EcgAcc ecg{0.0, -1, 0};
+  EcgAcc ecg{ecgMine, -1, 0};
   MinMaxAcc mm{__longlong_as_double(0x7ff0000000000000ll), -__longlong_as_double(0x7ff0000000000000ll), -1};
   for (int it = 0; t < a.nTiles; ++it, t += stride) {
     const int tn = t + stride;
@@ -738,6 +780,31 @@ __device__ __forceinline__ int64_t cell_voxel(int64_t i, const int64_t* __restri
   if (voxel) return voxel[i];
   const int64_t x = i % nx, y = (i / nx) % ny, z = i / ((int64_t)nx * ny);
   return (x + 1) + px * (y + py0) + pxy * (z + pz0);
+}
+
+// 1 / |r - p_j| for every cell and electrode, at the cell's slot
+// (invr[block][electrode][32], float when mixed); r = (x hx, y hy, z hz) as the step's
+// voxel decomposition gives it (ECGSensor's calcInvr_kernel,
+// elec/ECGSensor.cu:9-40).
+__global__ void ecg_invr_kernel(int64_t n, const int64_t* __restrict__ slot, const int64_t* __restrict__ voxel, int nx,
+                                int ny, int64_t px, int64_t pxy, int py0, int pz0, double hx, double hy, double hz,
+                                const double* __restrict__ pts, int nPts, int mixed, void* __restrict__ invr)
+{
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const int64_t vox = cell_voxel(c, voxel, nx, ny, px, pxy, py0, pz0);
+  const int64_t zz = vox / pxy, rem = vox - zz * pxy, yy = rem / px;
+  const double xr = (double)((int)(rem - yy * px) - 1) * hx;
+  const double yr = (double)((int)yy - py0) * hy;
+  const double zr = (double)((int)zz - pz0) * hz;
+  const int64_t i = slot[c], b = i / kBlk;
+  const int64_t at = b * nPts * kBlk + (i - b * kBlk);
+  for (int j = 0; j < nPts; ++j) {
+    const double ex = xr - pts[3 * j], ey = yr - pts[3 * j + 1], ez = zr - pts[3 * j + 2];
+    const double r = 1.0 / sqrt(ex * ex + ey * ey + ez * ez);
+    if (mixed) ((float*)invr)[at + j * kBlk] = (float)r;
+    else ((double*)invr)[at + j * kBlk] = r;
+  }
 }
 
 // Writes host-given Vm of cells c0 .. c0+n-1 into a padded block; sets
