@@ -216,9 +216,11 @@ class Engine:
         _lib.check(_lib.load().cdb_engine_step_host(self.h, tid, _lib.dptr(vm_in), _lib.dptr(vm_out)))
 
     def set_tuning(self, stage, ctas_per_sm):
-        """stage: 1 = copy each warp's next tile into shared memory while it
-        computes the current one; ctas_per_sm sizes the persistent grid
-        (0: as many CTAs per SM as are resident)."""
+        """stage: how each warp gets its next tile's inputs while it computes
+        the current one: 0 = direct loads, 1 = per-lane cp.async into shared
+        memory, 2 = bulk (TMA) copies into shared memory completing on an
+        mbarrier (defaults: 2 mixed, 0 FP64); ctas_per_sm sizes the
+        persistent grid (0: as many CTAs per SM as are resident)."""
         _lib.check(_lib.load().cdb_engine_set_tuning(self.h, int(stage), int(ctas_per_sm)))
 
     def get_tuning(self):
