@@ -22,6 +22,7 @@
 #include <omp.h>
 #include <cstdlib>
 #include <unistd.h>
+#include <dlfcn.h>
 
 #include "Anatomy.hh"
 #include "AnatomyCell.hh"
@@ -46,7 +47,8 @@ namespace {
 struct RefSim {
    Anatomy anatomy;
    ReactionManager reaction;
-   FGRDiffusionOMP* diffusion = nullptr;
+   Diffusion* diffusion = nullptr;
+   double diffusionScale = 0;
    std::vector<Stimulus*> stimulus;
    lazy_array<double> Vm, dVmR, dVmD, iStim;
    lazy_array<double> remote;
@@ -154,6 +156,7 @@ void* ref_sim_create(const char* reactionNames, const char* stimulusNames,
       for (long ii = 0; ii < nCells; ++ii) { v[ii] = 0; r[ii] = 0; d[ii] = 0; }
    }
    sim->reaction.initializeMembraneState(sim->Vm);
+   sim->diffusionScale = diffusionScale;
    if (sim->useDiffusion) {
       FGRUtils::FGRDiffusionParms p;
       p.printBBox_ = false;
@@ -165,6 +168,27 @@ void* ref_sim_create(const char* reactionNames, const char* stimulusNames,
    sim->actTime.assign(nCells, 0.0);
    sim->activated.assign(nCells, 0);
    return sim;
+}
+
+// Replaces the simulation's FGRDiffusionOMP by the Diffusion that the shared
+// library at `path` builds through its b200DiffusionFactory symbol (a
+// driver-side stand-in for the one-line diffusionFactory addition); 0 on
+// success.
+int ref_sim_use_diffusion_plugin(void* h, const char* path)
+{
+   RefSim* sim = static_cast<RefSim*>(h);
+   void* lib = dlopen(path, RTLD_NOW);
+   if (!lib) { std::fprintf(stderr, "dlopen %s: %s\n", path, dlerror()); return 1; }
+   typedef Diffusion* (*Factory)(const FGRUtils::FGRDiffusionParms&, const Anatomy&);
+   Factory f = (Factory)dlsym(lib, "b200DiffusionFactory");
+   if (!f) { std::fprintf(stderr, "dlsym b200DiffusionFactory: %s\n", dlerror()); return 2; }
+   FGRUtils::FGRDiffusionParms p;
+   p.printBBox_ = false;
+   p.diffusionScale_ = sim->diffusionScale;
+   delete sim->diffusion;
+   sim->diffusion = f(p, sim->anatomy);
+   sim->useDiffusion = true;
+   return 0;
 }
 
 void ref_sim_destroy(void* h)

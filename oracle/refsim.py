@@ -48,6 +48,8 @@ def lib():
         L.ref_sim_get_state.argtypes = [vp, ctypes.c_char_p, dp]
         L.ref_sim_set_state.argtypes = [vp, ctypes.c_char_p, dp]
         L.ref_sim_step.argtypes = [vp, ctypes.c_int]
+        L.ref_sim_use_diffusion_plugin.argtypes = [vp, ctypes.c_char_p]
+        L.ref_sim_use_diffusion_plugin.restype = ctypes.c_int
         L.ref_set_threads.argtypes = [ctypes.c_int]
         L.ref_read_pio.restype = ctypes.c_long
         L.ref_read_pio.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_int, dp,
@@ -116,6 +118,12 @@ class RefSim:
 
     def step(self, n=1):
         lib().ref_sim_step(self.h, n)
+
+    def use_diffusion_plugin(self, path):
+        """Replaces FGRDiffusionOMP by the Diffusion built by the library's
+        b200DiffusionFactory (the B200FGR adapter)."""
+        if lib().ref_sim_use_diffusion_plugin(self.h, path.encode()) != 0:
+            raise RuntimeError("ref_sim_use_diffusion_plugin failed for %s" % path)
 
     @property
     def time(self):

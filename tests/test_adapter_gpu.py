@@ -52,3 +52,59 @@ def test_adapter_in_reference_reaction_manager(cdb_lib):
     for name in ("Ca_i", "m", "h"):
         r = ref.state(name)
         assert np.abs(gpu.state(name) - r).max() <= 1e-8 * max(1e-12, np.abs(r).max())
+
+
+FGR_ADAPTER = os.path.join(ROOT, "oracle", "_ref", "libb200fgr.so")
+
+
+def _holed(t):
+    """The tissue with a block of cells removed (anatomy holes: the stencil
+    sees non-tissue neighbours)."""
+    x, y, z = t.tuples()
+    keep = ~((x >= 3) & (x < 6) & (y >= 2) & (y < 5) & (z >= 1) & (z < 4))
+    return tissue.Tissue(t.nx, t.ny, t.nz, t.dx, t.dy, t.dz, t.gid[keep], t.cell_type[keep], t.sigma[keep],
+                         t.vm0[keep], t.stimuli)
+
+
+def _b200_reaction_sim(t):
+    """A RefSim whose three reactions are the B200TT06 adapter (loaded by
+    the reference's reactionFactory) on the shipped fits."""
+    from golden.make_golden import reference_sim
+    from oracle import refsim
+    reference_sim(t).close()          # compiles the shipped fits into the object database
+    text = ""
+    for name, ct, fit in (("b200Endo", 0, "tt06Endo_fit"), ("b200Mid", 1, "tt06Mid_fit"), ("b200Epi", 2, "tt06Epi_fit")):
+        text += "%s REACTION { method = %s; cellTypes = %d; celltype = %d; fit = %s; }\n" % (name, ADAPTER, 100 + ct,
+                                                                                          ct, fit)
+    refsim.compile_once("b200-adapter", text)
+    prefix = refsim.unique_prefix()
+    refsim.compile_objects(tissue.stimulus_objects_text(t.stimuli, prefix=prefix))
+    return refsim.RefSim(["b200Endo", "b200Mid", "b200Epi"], ["%s%d" % (prefix, i) for i in range(len(t.stimuli))],
+                         (t.nx, t.ny, t.nz), (t.dx, t.dy, t.dz), t.gid, t.cell_type, t.sigma, 0.02,
+                         t.diffusion_scale)
+
+
+@pytest.mark.skipif(not (_built() and os.path.exists(FGR_ADAPTER)), reason="oracle/_ref with the adapters not built")
+@pytest.mark.parametrize("holes,reactions", [(False, "reference"), (True, "reference"), (True, "b200")])
+def test_fgr_adapter_in_reference_time_loop(cdb_lib, holes, reactions):
+    """The B200FGR Diffusion adapter (cardioid_b200/adapter/B200FGR.cc) in
+    place of the reference's FGRDiffusionOMP inside its own time loop, with
+    the reference's BetterTT06 or with the B200TT06 reaction adapter (the
+    whole step then on the GPU through the two adapters): FP64 max |dVm| <=
+    1e-6 mV after 300 steps against the all-reference simulation, identical
+    activation times."""
+    from golden.make_golden import reference_sim
+    t = tissue.box(10, 8, 6, dx=0.2, seed=23)
+    if holes:
+        t = _holed(t)
+    ref = reference_sim(t)
+    gpu = reference_sim(t) if reactions == "reference" else _b200_reaction_sim(t)
+    gpu.use_diffusion_plugin(FGR_ADAPTER)
+    for s in (ref, gpu):
+        s.set_vm(t.vm0)
+    for _ in range(3):
+        ref.step(100)
+        gpu.step(100)
+    assert np.abs(gpu.vm() - ref.vm()).max() <= 1e-6
+    np.testing.assert_array_equal(gpu.activation(), ref.activation())
+    assert (ref.activation() > 0).any()
