@@ -983,7 +983,9 @@ cdb_status cdb_engine_sync(cdb_engine* e)
   CDB_CUDA(cudaMemcpy(&err, e->e.dErr.p, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) {
     CDB_CUDA(cudaMemset(e->e.dErr.p, 0, sizeof(int)));
-    CDB_CHECK(false, (cdb_status)err, "a bounded wait in the step kernel gave up (its copies did not arrive)");
+    CDB_CHECK(false, (cdb_status)err,
+              err == CDB_NUMERIC_FAULT ? "a non-finite Vm was found at the end of a launch batch"
+                                       : "a bounded wait in the step kernel gave up (its copies did not arrive)");
   }
   return CDB_OK;
 }

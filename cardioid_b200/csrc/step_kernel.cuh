@@ -24,6 +24,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cfloat>
+
 #include "common.cuh"
 #include "fgr_device.cuh"
 #include "tt06_step.cuh"
@@ -502,6 +504,9 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
     if (active) {
       mm.lo = fmin(mm.lo, vnew);
       mm.hi = fmax(mm.hi, vnew);
+      // a non-finite Vm stays non-finite, so checking at the batch's last
+      // step catches it; the first error recorded is kept
+      if (!(fabs(vnew) <= DBL_MAX)) atomicCAS(a.err, 0, (int)CDB_NUMERIC_FAULT);
     }
   }
   // ECG (ECGSensor::eval / calcEcg, elec/ECGSensor.cc:231-320 and

@@ -225,7 +225,9 @@ cdb_status cdb_engine_remove_tissue(cdb_engine* e, int32_t id);
 cdb_status cdb_engine_step(cdb_engine* e, int32_t nSteps);
 /* Blocks until the engine's stream is idle; CDB_TIMEOUT if a bounded wait
  * inside the step gave up since the last call (the affected steps are
- * incomplete). */
+ * incomplete); CDB_NUMERIC_FAULT if a cell's Vm was NaN or infinite at the
+ * end of a launch batch of cdb_engine_step (checked with the min/max
+ * sensor, on each batch's last step). */
 cdb_status cdb_engine_sync(cdb_engine* e);
 /* Number of steps a tissue has taken and its time (ms, accumulated as
  * time += dt like the reference). */

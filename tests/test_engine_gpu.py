@@ -393,3 +393,28 @@ def test_tiny_and_ragged_tissues_match_oracle(cdb_lib, oracle_port, fits002, sha
     assert np.abs(vm - sim.vm()).max() <= VM_TOL_FP64
     np.testing.assert_array_equal(act, sim.activation())
     assert (act > 0).any()
+
+
+def test_non_finite_vm_reported_by_sync(cdb_lib, fits002):
+    """A NaN that the host writes into Vm (the failure is made on the host;
+    NaN arithmetic faults nothing on the device) is reported by
+    cdb_engine_sync as CDB_NUMERIC_FAULT after the next launch batch, once;
+    a clean engine's sync stays OK."""
+    from cardioid_b200 import _lib
+    t = tissue.box(12, 10, 8)
+    with _engine(fits002) as e:
+        tid = e.add_tissue(t, _reaction_ids(t))
+        e.step(10)
+        e.sync()
+        vm = e.read_vm(tid)
+        vm[5] = np.nan
+        e.write_vm(tid, vm)
+        e.step(10)
+        with pytest.raises(_lib.CdbError) as err:
+            e.sync()
+        assert err.value.status == _lib.CDB_NUMERIC_FAULT
+        e.sync()                      # read once, then cleared
+    with _engine(fits002) as e:
+        e.add_tissue(t, _reaction_ids(t))
+        e.step(50)
+        e.sync()
