@@ -201,3 +201,22 @@ def test_server_builds_on_worker_threads_with_the_same_results():
         out[workers] = sorted((r.id, r.cells, r.steps, r.activated, tuple(r.activation)) for r in res)
     assert out[0] == out[2]
     assert [r[0] for r in out[0]] == [j.id for j in jobs]
+
+
+def test_server_build_errors_reach_the_caller():
+    """A tissue that fails to build on a worker thread raises from run(), and
+    the workers are shut down."""
+    jobs = _jobs(n=6, seed=3)
+    bad = jobs[2].id
+
+    def build(inst):
+        if inst.index == bad:
+            raise ValueError("no tissue for instance %d" % inst.index)
+        return FakeTissue(inst)
+
+    eng = FakeEngine(total=100 * 120000)
+    srv = serving.Server(eng, [0, 1, 2], clock=eng.clock, sleep=lambda s: setattr(eng, "now", eng.now + s),
+                         build=build, reserve=0, workers=2)
+    with pytest.raises(ValueError, match="no tissue"):
+        srv.run(jobs)
+    assert srv._pool is None
