@@ -305,7 +305,7 @@ def run_ours(args):
     errors = {"steps": int(sf), "max_abs_dvm_mV": float(np.abs(vm_ - vf).max()),
               "activated_fp64": int((af > 0).sum()), "activated_mixed": int((am > 0).sum()),
               "activation_max_err_ms": float(np.abs(af[both] - am[both]).max()) if both.any() else None,
-              "apd90": "beats last 300 ms, past this window; tests/test_engine_gpu.py checks APD90 on a full beat"}
+              "full_beat": apd_check(local) if world == 1 and not args.no_apd else None}
     plain = time_plain_fp64(t, args, local) if world == 1 and not args.no_plain else None
     line = {
         "metric": METRIC, "value": m["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -425,6 +425,40 @@ def run_serve(args):
                           "%d steps each at dt %g" % (args.jobs, args.rate, args.job_steps, DT), **out}), flush=True)
 
 
+def apd_check(local, n=32, steps=20000, every=10, probes=64):
+    """Mixed against FP64 over one full paced beat (400 ms) of an n^3 box:
+    Vm sampled every `every` steps at `probes` cells spread over the box,
+    APD90 per probe (cardioid_b200.sensors.apd90), activation times of every
+    cell; the largest differences."""
+    from cardioid_b200 import engine, sensors, tissue
+    t = tissue.box(n, n, n, period=1000.0, seed=99)
+    idx = np.linspace(0, t.n - 1, probes).astype(np.int64)
+    tr, act = {}, {}
+    times = DT * every * np.arange(1, steps // every + 1)
+    for prec in ("fp64", "mixed"):
+        with engine.Engine(DT, precision=prec, device=local) as e:
+            rx, _ = engine.transmural_setup(e, t, DT)
+            tid = e.add_tissue(t, rx)
+            rows = []
+            for _ in range(steps // every):
+                e.step(every)
+                rows.append(e.read_vm(tid)[idx])
+            tr[prec], act[prec] = np.array(rows), e.read_activation(tid)
+    errs, apds = [], []
+    for j in range(probes):
+        a64, am = sensors.apd90(tr["fp64"][:, j], times), sensors.apd90(tr["mixed"][:, j], times)
+        if len(a64) and len(a64) == len(am):
+            errs.append(float(np.abs(a64 - am).max()))
+            apds.append(float(a64.mean()))
+    both = (act["fp64"] > 0) & (act["mixed"] > 0)
+    return {"workload": "%d^3 box, one paced beat (%d steps, %g ms), Vm sampled every %d steps at %d probe cells"
+                        % (n, steps, steps * DT, every, probes),
+            "apd90_probes": len(errs), "apd90_max_err_ms": max(errs) if errs else None,
+            "apd90_mean_fp64_ms": float(np.mean(apds)) if apds else None,
+            "activation_max_err_ms": float(np.abs(act["fp64"] - act["mixed"])[both].max()) if both.any() else None,
+            "activated_fp64": int((act["fp64"] > 0).sum()), "activated_mixed": int((act["mixed"] > 0).sum())}
+
+
 def time_plain_fp64(t, args, local):
     """The plain FP64 GPU path: the reference's split loop on the drop-in
     plugins (elec/simulationLoop.cc:183-231), one Reaction::calc per
@@ -507,6 +541,7 @@ def main():
     ap.add_argument("--precision", choices=["both", "fp64", "mixed"], default="both",
                     help="profiling runs: time one precision only (no headline line)")
     ap.add_argument("--no-e2e", action="store_true", help="profiling runs: skip the end-to-end loop")
+    ap.add_argument("--no-apd", action="store_true", help="skip the full-beat APD90 comparison (mixed vs FP64)")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 plugin path")
     args = ap.parse_args()
     if args.warmup < 3:

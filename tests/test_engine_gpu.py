@@ -12,6 +12,7 @@ import pytest
 
 from cardioid_b200 import engine as eng_mod
 from cardioid_b200 import tissue, tt06
+from cardioid_b200.sensors import apd90
 
 pytestmark = pytest.mark.gpu
 
@@ -256,22 +257,6 @@ def test_point_and_box_stimuli_match_oracle(cdb_lib, oracle_port, fits002, preci
         both = (act > 0) & (ref_act > 0)
         assert (both == (ref_act > 0)).all()
         assert np.abs(act[both] - ref_act[both]).max() <= ACT_TOL_MIXED
-
-
-def apd90(trace, times):
-    """APD90 per beat of one cell's Vm trace: activation at the first step
-    with Vm > 0, V_rest = Vm just before it, V_peak the maximum after it;
-    repolarisation when Vm first falls below V_rest + 0.1 (V_peak - V_rest)."""
-    up = np.flatnonzero((trace[1:] > 0) & (trace[:-1] <= 0)) + 1
-    out = []
-    for u in up:
-        vrest = trace[u - 1]
-        peak_i = u + np.argmax(trace[u:])
-        thr = vrest + 0.1 * (trace[peak_i] - vrest)
-        below = np.flatnonzero(trace[peak_i:] < thr)
-        if len(below):
-            out.append(times[peak_i + below[0]] - times[u])
-    return np.array(out)
 
 
 def test_mixed_precision_errors_vs_fp64_oracle(cdb_lib, oracle_port, fits002):
