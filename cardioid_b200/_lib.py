@@ -120,6 +120,7 @@ def load():
         "cdb_engine_remove_tissue": (st, [vp, ctypes.c_int32]),
         "cdb_engine_step": (st, [vp, ctypes.c_int32]),
         "cdb_engine_sync": (st, [vp]),
+        "cdb_engine_test_bounded_wait": (st, [vp]),
         "cdb_engine_tissue_time": (st, [vp, ctypes.c_int32, i64p, dp]),
         "cdb_engine_set_clock": (st, [vp, ctypes.c_int32, ctypes.c_int64, ctypes.c_double]),
         "cdb_engine_set_ecg": (st, [vp, ctypes.c_int32, ctypes.c_int32, dp, ctypes.c_int32, ctypes.c_double]),

@@ -188,6 +188,7 @@ struct Engine {
   bool graphMinmax = false;
   // launch tuning (cdb_engine_set_tuning; the autotuner picks them)
   int stage = 1;           // 1: stage each warp's next tile through shared memory (cp.async)
+  bool withhold = false;   // cdb_engine_test_bounded_wait: the next batch withholds its bulk copies
   int ctasPerSm = 0;       // persistent grid: SMs x this; 0 = as many as are resident
   int numSms = 148;
   int resident[2][CDB_MAX_REACTION_TYPES + 1] = {};   // resident CTAs per SM by [ECG][slot] (last: generic)
@@ -359,8 +360,9 @@ struct Engine {
     a.dt = cfg.dt;
     a.k = s;
     a.minmax = minmax ? 1 : 0;
-    a.stage = stage;
+    a.stage = withhold ? 2 : stage;
     a.err = dErr.as<int>();
+    a.withhold = withhold ? 1 : 0;
     const int slot = spec[rt] ? rt : -1;
     const unsigned grid = (unsigned)std::min<int64_t>(grid_for(a.nTiles, kWarpsPerCta),
                                                       (int64_t)numSms * grid_ctas_per_sm(slot));
@@ -392,6 +394,14 @@ struct Engine {
     if (st != CDB_OK) return st;
     st = rebuild();
     if (st != CDB_OK) return st;
+    if (withhold) {
+      // one batch, launched directly (never captured), then back to normal
+      launch_batch(k, minmax);
+      withhold = false;
+      CDB_CUDA(cudaGetLastError());
+      advance_host(k);
+      return CDB_OK;
+    }
     if (cfg.use_graphs) {
       if (!graph || graphSteps != k || graphMinmax != minmax) {
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
@@ -1343,6 +1353,13 @@ cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, 
   CDB_CUDA(cudaGetLastError());
   CDB_CUDA(cudaStreamSynchronize(E.sOut));
   CDB_CUDA(cudaStreamSynchronize(s));
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_test_bounded_wait(cdb_engine* e)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  e->e.withhold = true;
   return CDB_OK;
 }
 

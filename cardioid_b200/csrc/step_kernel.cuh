@@ -119,6 +119,7 @@ struct StepArgs {
   int minmax;                 // reduce min/max this step
   int stage;                  // 1: stage the next tile through shared memory (cp.async), 2: with bulk copies
   int* err;                   // set to CDB_TIMEOUT when a bounded wait gives up
+  int withhold;               // test of the bounded waits (stage 2): issue no copies after each warp's first tile
 };
 
 __constant__ TT06Scalars c_scal[CDB_MAX_REACTION_TYPES];
@@ -342,13 +343,25 @@ __device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned b
                : "memory");
 }
 
-// Bounded wait for a buffer's copies (every lane): false after about 2^20
-// polls, each of which the hardware may suspend for a while.
+// Bounded wait for a buffer's copies (every lane): false once about a
+// second has passed on the GPU's global timer (checked every 64 polls), or
+// after 2^20 polls, each of which the hardware may suspend for a while.
 constexpr int kWaitPolls = 1 << 20;
+constexpr unsigned long long kWaitNs = 1000000000ull;
+__device__ __forceinline__ unsigned long long global_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity)
 {
-  for (int i = 0; i < kWaitPolls; ++i)
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (int i = 0; i < kWaitPolls; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63) == 63 && global_ns() - t0 > kWaitNs) return false;
+  }
   return false;
 }
 
@@ -621,7 +634,7 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
       }
       __syncwarp();           // every lane is past the wait and done with the other buffer
       const WarpTile nxt = tn < a.nTiles ? *(bi ? desc1 : desc0) : WarpTile{};
-      if (tn < a.nTiles && lane == 0)
+      if (tn < a.nTiles && lane == 0 && !a.withhold)
         stage_tile_bulk<MIXED>(a, nxt, mine + (bi ^ 1) * kBuf,
                                tn + stride < a.nTiles ? a.tiles + tn + stride : nullptr, bi ? desc0 : desc1,
                                bars + (bi ^ 1));

@@ -145,6 +145,12 @@ class Engine:
     def sync(self):
         _lib.check(_lib.load().cdb_engine_sync(self.h))
 
+    def test_bounded_wait(self):
+        """The next step batch withholds its bulk copies after each warp's
+        first tile, so its bounded waits run out (about a second) and sync
+        raises a CdbError with status TIMEOUT; for testing the failure path."""
+        _lib.check(_lib.load().cdb_engine_test_bounded_wait(self.h))
+
     def time(self, tid):
         s, t = ctypes.c_int64(), ctypes.c_double()
         _lib.check(_lib.load().cdb_engine_tissue_time(self.h, tid, ctypes.byref(s), ctypes.byref(t)))

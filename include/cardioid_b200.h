@@ -229,6 +229,12 @@ cdb_status cdb_engine_step(cdb_engine* e, int32_t nSteps);
  * end of a launch batch of cdb_engine_step (checked with the min/max
  * sensor, on each batch's last step). */
 cdb_status cdb_engine_sync(cdb_engine* e);
+/* Test of the failure path (no counterpart in the reference): the next
+ * cdb_engine_step batch runs with bulk-copy staging and issues no copies
+ * after each warp's first tile, so those warps' bounded waits (about a
+ * second each) run out, the batch is left incomplete and cdb_engine_sync
+ * returns CDB_TIMEOUT; nothing faults, and later batches run normally. */
+cdb_status cdb_engine_test_bounded_wait(cdb_engine* e);
 /* Number of steps a tissue has taken and its time (ms, accumulated as
  * time += dt like the reference). */
 cdb_status cdb_engine_tissue_time(cdb_engine* e, int32_t id, int64_t* steps, double* time);

@@ -403,3 +403,26 @@ def test_non_finite_vm_reported_by_sync(cdb_lib, fits002):
         e.add_tissue(t, _reaction_ids(t))
         e.step(50)
         e.sync()
+
+
+def test_bounded_wait_runs_out_and_engine_recovers(cdb_lib, fits002):
+    """The failure path of the step's bounded waits, made without a fault:
+    one batch withholds its bulk copies after each warp's first tile (a wait
+    that nothing completes), its waits give up after about a second, the
+    warps leave, and cdb_engine_sync reports CDB_TIMEOUT; the next batches
+    run normally on the same context."""
+    from cardioid_b200 import _lib
+    t = tissue.box(96, 96, 96)          # about 9000 tiles per type: several per warp
+    with eng_mod.Engine(DT, precision="mixed") as e:
+        rx, _ = eng_mod.transmural_setup(e, t, DT)
+        tid = e.add_tissue(t, rx)
+        e.step(5)
+        e.sync()
+        e.test_bounded_wait()
+        e.step(1)
+        with pytest.raises(_lib.CdbError) as err:
+            e.sync()
+        assert err.value.status == _lib.CDB_TIMEOUT
+        e.step(20)
+        e.sync()
+        assert np.isfinite(e.read_vm(tid)).all()
