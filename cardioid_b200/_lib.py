@@ -14,8 +14,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("CARDIOID_B200_LIB") or os.path.join(HERE, "_lib", "libcardioid_b200.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "cardioid_b200.h")
 
-CDB_OK, CDB_INVALID_ARG, CDB_OOM, CDB_CUDA_ERROR, CDB_NUMERIC_FAULT, CDB_TIMEOUT, CDB_NOT_FOUND = range(7)
-STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "NUMERIC_FAULT", 5: "TIMEOUT", 6: "NOT_FOUND"}
+CDB_OK, CDB_INVALID_ARG, CDB_OOM, CDB_CUDA_ERROR, CDB_NUMERIC_FAULT, CDB_TIMEOUT, CDB_NOT_FOUND, CDB_BOUNDS_FAULT = range(8)
+STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "OOM", 3: "CUDA_ERROR", 4: "NUMERIC_FAULT", 5: "TIMEOUT", 6: "NOT_FOUND",
+                7: "BOUNDS_FAULT"}
 CDB_FP64, CDB_MIXED = 0, 1
 NUM_FITS, NUM_STATES, MAX_COEFF = 30, 18, 64
 MAX_REACTION_TYPES, MAX_STIM_PER_TISSUE = 6, 32

@@ -375,6 +375,8 @@ struct Engine {
     a.stage = withhold ? 2 : stage;
     a.err = dErr.as<int>();
     a.withhold = withhold ? 1 : 0;
+    a.nTissues = (int)order.size();
+    a.nTimes = (int64_t)(dTimes.bytes / sizeof(double));
     const int slot = spec[rt] ? rt : -1;
     const unsigned grid = (unsigned)std::min<int64_t>(grid_for(a.nTiles, kWarpsPerCta),
                                                       (int64_t)numSms * grid_ctas_per_sm(slot));
@@ -953,6 +955,8 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
   d.actAll = 1;
   d.hx = t->dx; d.hy = t->dy; d.hz = t->dz;
   d.vrel = h->vrel.as<int>();
+  d.nSlots = nSlots;
+  d.nVox = vox;
   init_state_kernel<<<grid_for(nSlots, 256), 256, 0, s>>>(nSlots, d.s64, d.s32, mixed ? 1 : 0, d.act);
   E.launches += 1;
   {
@@ -1008,8 +1012,9 @@ cdb_status cdb_engine_sync(cdb_engine* e)
   if (err) {
     CDB_CUDA(cudaMemset(e->e.dErr.p, 0, sizeof(int)));
     CDB_CHECK(false, (cdb_status)err,
-              err == CDB_NUMERIC_FAULT ? "a non-finite Vm was found at the end of a launch batch"
-                                       : "a bounded wait in the step kernel gave up (its copies did not arrive)");
+              err == CDB_NUMERIC_FAULT  ? "a non-finite Vm was found at the end of a launch batch"
+              : err == CDB_BOUNDS_FAULT ? "the bounds-checked build found an index out of range"
+                                        : "a bounded wait in the step kernel gave up (its copies did not arrive)");
   }
   return CDB_OK;
 }

@@ -45,6 +45,7 @@ struct TissueDev {
   const int* vrel;         // per slot: voxel offset from its tile's vox0
   double* act;             // per slot
   int64_t n;
+  int64_t nSlots, nVox;   // sizes of the slot arrays and of each padded Vm block (checked builds)
   int64_t px, pxy;        // padded strides
   int nx, ny, nz;
   int py0, pz0;           // 1 when y (z) is padded
@@ -120,6 +121,28 @@ struct StepArgs {
   int stage;                  // 1: stage the next tile through shared memory (cp.async), 2: with bulk copies
   int* err;                   // set to CDB_TIMEOUT when a bounded wait gives up
   int withhold;               // test of the bounded waits (stage 2): issue no copies after each warp's first tile
+  int nTissues;               // sizes of the tissue and time tables (checked builds)
+  int64_t nTimes;
+};
+
+// Index guard of the checked build (compiled with CDB_BOUNDS_CHECK, the
+// stand-in for a memory checker on a pool where compute-sanitizer is
+// closed): an index outside [0, n) records CDB_BOUNDS_FAULT in the engine's
+// error word (cdb_engine_sync returns it) and is replaced by 0, so the
+// access stays inside the array.  In the normal build it is the identity.
+struct IndexCheck {
+  int64_t n;
+  int* err;
+  __device__ __forceinline__ int64_t operator()(int64_t i) const
+  {
+#ifdef CDB_BOUNDS_CHECK
+    if ((unsigned long long)i >= (unsigned long long)n) {
+      atomicCAS(err, 0, (int)CDB_BOUNDS_FAULT);
+      return 0;
+    }
+#endif
+    return i;
+  }
 };
 
 __constant__ TT06Scalars c_scal[CDB_MAX_REACTION_TYPES];
@@ -162,13 +185,14 @@ __device__ __forceinline__ int64_t node_offset(int64_t px, int64_t pxy, int node
 // at the cell's row-0 weight, rows kBlk apart.
 template <int CLS>
 __device__ __forceinline__ double stencil64(const double* __restrict__ w, int64_t px, int64_t pxy,
-                                            const double* __restrict__ vin, int64_t vox, double phi0)
+                                            const double* __restrict__ vin, int64_t vox, double phi0,
+                                            const IndexCheck& vchk)
 {
   double tmp = __ldg(w) * phi0;
 #pragma unroll
   for (int r = 1; r < class_rows(CLS); ++r) {
     const int node = class_node(CLS, r);
-    tmp += __ldg(w + r * kBlk) * __ldg(vin + vox + node_offset(px, pxy, node));
+    tmp += __ldg(w + r * kBlk) * __ldg(vin + vchk(vox + node_offset(px, pxy, node)));
   }
   return tmp;
 }
@@ -177,13 +201,14 @@ __device__ __forceinline__ double stencil64(const double* __restrict__ w, int64_
 // memory); the differences are taken in FP64 (A0 = -sum A_k).
 template <int CLS>
 __device__ __forceinline__ double stencil32(const float* __restrict__ w, int64_t px, int64_t pxy,
-                                            const double* __restrict__ vin, int64_t vox, double phi0)
+                                            const double* __restrict__ vin, int64_t vox, double phi0,
+                                            const IndexCheck& vchk)
 {
   float tmp = 0.f;
 #pragma unroll
   for (int r = 1; r < class_rows(CLS); ++r) {
     const int node = class_node(CLS, r);
-    const float d = (float)(__ldg(vin + vox + node_offset(px, pxy, node)) - phi0);
+    const float d = (float)(__ldg(vin + vchk(vox + node_offset(px, pxy, node))) - phi0);
     tmp = fmaf(w[(r - 1) * kBlk], d, tmp);
   }
   return (double)tmp;
@@ -241,8 +266,8 @@ __device__ __forceinline__ void stage_desc(const WarpTile* src, WarpTile* dst, i
 template <bool MIXED>
 __device__ __forceinline__ void stage_tile(const StepArgs& a, const WarpTile& tile, int lane, unsigned char* buf)
 {
-  const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
-  const int64_t b = tile.first / kBlk;
+  const TissueDev* __restrict__ Tp = a.tissues + IndexCheck{a.nTissues, a.err}(tile.tissue);
+  const int64_t b = IndexCheck{Tp->nSlots, a.err}(tile.first) / kBlk;
   if (MIXED) {
     warp_copy(buf, (const unsigned char*)(Tp->s64 + b * kRowsMixed64 * kBlk), kRowsMixed64 * kBlk * 8, lane);
     warp_copy(buf + kRowsMixed64 * kBlk * 8, (const unsigned char*)(Tp->s32 + b * kRowsMixed32 * kBlk),
@@ -372,8 +397,8 @@ template <bool MIXED>
 __device__ __forceinline__ void stage_tile_bulk(const StepArgs& a, const WarpTile& tile, unsigned char* buf,
                                                 const WarpTile* nextDesc, WarpTile* descDst, unsigned long long* bar)
 {
-  const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
-  const int64_t b = tile.first / kBlk;
+  const TissueDev* __restrict__ Tp = a.tissues + IndexCheck{a.nTissues, a.err}(tile.tissue);
+  const int64_t b = IndexCheck{Tp->nSlots, a.err}(tile.first) / kBlk;
   unsigned bytes = kBlk * 4 + (nextDesc ? 32u : 0u);
   int wr = 0;
   if (MIXED) {
@@ -405,16 +430,18 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
                                           bool staged, EcgAcc& ecg, MinMaxAcc& mm)
 {
   constexpr bool SPEC = SLOT >= 0;
-  const TissueDev* __restrict__ Tp = a.tissues + tile.tissue;
+  const TissueDev* __restrict__ Tp = a.tissues + IndexCheck{a.nTissues, a.err}(tile.tissue);
+  const IndexCheck tchk{a.nTimes, a.err};
   const int64_t lstep = Tp->step0 + a.k;
-  const double time = a.times[Tp->timeOff + lstep];
-  const double tnext = a.times[Tp->timeOff + lstep + 1];
+  const double time = a.times[tchk(Tp->timeOff + lstep)];
+  const double tnext = a.times[tchk(Tp->timeOff + lstep + 1)];
   const bool active = lane < tile.count;
   // lanes past the tile's end stand in for its first cell until the end
   const int l = active ? lane : 0;
-  const int64_t i = tile.first + l;
+  const IndexCheck schk{Tp->nSlots, a.err}, vchk{Tp->nVox, a.err};
+  const int64_t i = schk(tile.first + l);
   const int rel = staged ? ((const int*)(buf + vrel_offset<MIXED>()))[l] : Tp->vrel[i];
-  const int64_t vox = tile.vox0 + rel;
+  const int64_t vox = vchk(tile.vox0 + rel);
   const int64_t px = Tp->px, pxy = Tp->pxy;
   // iStim = 0, then the stimuli whose boxes hold a cell of the tile, in order
   double istim = 0.0;
@@ -454,15 +481,15 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
         const int wr = weight_rows(cls, true);
         const float* w = staged ? (const float*)(buf + kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4) + pos
                                 : (const float*)Tp->w + b * wr * kBlk + pos;
-        acc = cls == kVolume ? stencil32<kVolume>(w, px, pxy, vin, vox, phi0)
-            : cls == kSheet ? stencil32<kSheet>(w, px, pxy, vin, vox, phi0)
-                            : stencil32<kCable>(w, px, pxy, vin, vox, phi0);
+        acc = cls == kVolume ? stencil32<kVolume>(w, px, pxy, vin, vox, phi0, vchk)
+            : cls == kSheet ? stencil32<kSheet>(w, px, pxy, vin, vox, phi0, vchk)
+                            : stencil32<kCable>(w, px, pxy, vin, vox, phi0, vchk);
       } else {
         const int wr = weight_rows(cls, false);
         const double* w = (const double*)Tp->w + b * wr * kBlk + pos;
-        acc = cls == kVolume ? stencil64<kVolume>(w, px, pxy, vin, vox, phi0)
-            : cls == kSheet ? stencil64<kSheet>(w, px, pxy, vin, vox, phi0)
-                            : stencil64<kCable>(w, px, pxy, vin, vox, phi0);
+        acc = cls == kVolume ? stencil64<kVolume>(w, px, pxy, vin, vox, phi0, vchk)
+            : cls == kSheet ? stencil64<kSheet>(w, px, pxy, vin, vox, phi0, vchk)
+                            : stencil64<kCable>(w, px, pxy, vin, vox, phi0, vchk);
       }
       dvmD = acc * scale;
     }

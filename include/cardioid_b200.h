@@ -35,7 +35,8 @@ typedef enum {
   CDB_CUDA_ERROR = 3,    /* a CUDA runtime call or kernel launch failed */
   CDB_NUMERIC_FAULT = 4, /* a non-finite Vm was detected */
   CDB_TIMEOUT = 5,       /* a bounded device wait gave up */
-  CDB_NOT_FOUND = 6      /* no tissue or reaction with that id */
+  CDB_NOT_FOUND = 6,     /* no tissue or reaction with that id */
+  CDB_BOUNDS_FAULT = 7   /* the bounds-checked build found an index out of range */
 } cdb_status;
 
 typedef enum { CDB_FP64 = 0, CDB_MIXED = 1 } cdb_precision;
