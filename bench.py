@@ -73,16 +73,19 @@ def read_traffic(precision):
 
 def _cpu_worker(args):
     """Runs the reference CPU path (oracle/_ref) or the oracle port on one
-    sample box; returns (cells, steps, seconds)."""
-    kind, shape, steps, warmup, seed = args
-    os.environ["OMP_NUM_THREADS"] = "1"
+    sample box with `threads` OpenMP threads (the reference's omp loop: the
+    FGR stencil threaded, BetterTT06 single-threaded); returns (cells,
+    steps, seconds)."""
+    kind, shape, steps, warmup, seed = args[:5]
+    threads = args[5] if len(args) > 5 else 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from cardioid_b200 import engine, tissue
     t = tissue.box(*shape, seed=seed)
     if kind == "reference":
         from golden.make_golden import reference_sim
         from oracle import refsim
-        refsim.set_threads(1)
+        refsim.set_threads(threads)
         sim = reference_sim(t)
         sim.set_vm(t.vm0)
     else:
@@ -116,9 +119,15 @@ def cpu_baseline(steps, warmup, procs=None):
     what = ("the reference's own CPU path (oracle/_ref: BetterTT06 + FGRDiffusionOMP + BoxStimulus, omp-loop order)"
             if kind == "reference" else "the oracle's C restatement of the reference path")
     per_core = sum(r[0] * r[1] / r[2] for r in res) / len(res)
+    # the reference as it runs: one process, the stencil on every core
+    with ctx.Pool(1) as pool:
+        n1, s1, w1 = pool.map(_cpu_worker, [(kind, CPU_SAMPLE, steps, warmup, 100, procs)])[0]
     return {"value": cells / wall, "unit": METRIC, "cores": procs, "kind": kind, "per_core": per_core,
+            "omp_loop_one_process": n1 * s1 / w1,
             "sample": "%s; %d processes (one per host core, like one MPI rank per core, no halo exchange), "
-                      "each a %dx%dx%d box of the same workload for %d steps after %d warm-up; CPU: %s"
+                      "each a %dx%dx%d box of the same workload for %d steps after %d warm-up; "
+                      "omp_loop_one_process: one process on the same box with the stencil's OpenMP loop on every "
+                      "core and the reaction on one, as the reference's omp loop runs; CPU: %s"
                       % (what, procs, CPU_SAMPLE[0], CPU_SAMPLE[1], CPU_SAMPLE[2], steps, warmup, cpu)}
 
 
