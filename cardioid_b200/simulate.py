@@ -1,0 +1,244 @@
+"""Runs a Cardioid object.data deck on the fused engine: the caller side of
+the hot path, as the reference's set-up (elec/initializeSimulate.cc) and
+omp time loop (elec/simulationLoop.cc:150-243) use it.
+
+    sim = simulate.load(["object.data", "tt06.fit.data"])
+    out = sim.run(precision="fp64")          # maxLoop steps
+    out["vm"], out["activation"], out["minmax"], out["print"]
+
+    python -m cardioid_b200.simulate object.data tt06.fit.data --precision mixed --out run.npz
+
+What a deck may hold, per class (keys and defaults as the reference reads
+them):
+  SIMULATE     anatomy, diffusion, reaction (list), stimulus (list), sensor
+               (list), dt, maxLoop, loop, time, printRate, printGid
+  ANATOMY      method = brick (cellType, dx dy dz, xSize ySize zSize or nx
+               ny nz; elec/initializeAnatomy.cc:147-239) or pio (fileName;
+               cardioid_b200.anatomy.read_anatomy), conductivity
+  CONDUCTIVITY method = uniform (sigma11 sigma22 sigma33 sigma12 sigma13
+               sigma23) or fibre (sigmaLi, sigmaTi: read with the pio
+               anatomy's angles)
+  DIFFUSION    method = FGR (any variant) or b200, diffusionScale; method
+               null runs without diffusion
+  REACTION     method = BetterTT06 (cardioid_b200.tt06.params_from_object),
+               cellTypes; SINGLECELL objects named by a reaction set its
+               cells' initial state
+  STIMULUS     method = box (xMin..zMax, elec/stimulusFactory.cc:96-110) or
+               point (cell: a local cell index), pulse = periodic (vStim,
+               tStart, duration, period, t0, tf)
+  SENSOR       method = activationTime or minMax: their results come back
+               from run()
+Other methods raise ValueError (no silent substitution).
+"""
+import argparse
+import os
+
+import numpy as np
+
+from . import anatomy as anatomy_mod
+from . import objectdb, tissue, tt06
+
+
+class Simulation:
+    """A deck turned into engine inputs: tissue, reaction parameters and
+    per-cell reaction ids, initial states, dt and step count."""
+
+    def __init__(self, t, params, reaction_of_cell, states, dt, steps, sensors, print_rate, print_gid):
+        self.tissue = t
+        self.params = params
+        self.reaction_of_cell = reaction_of_cell
+        self.states = states                  # None, or 18 x n initial states
+        self.dt = dt
+        self.steps = steps
+        self.sensors = sensors
+        self.print_rate = print_rate
+        self.print_gid = print_gid
+
+    def run(self, precision="fp64", steps=None, device=0):
+        """Runs the deck's steps (or `steps`) on the fused engine and returns
+        Vm, activation times, min/max Vm and the printed rows (loop, time,
+        gid, Vm every printRate steps, as the reference's printData)."""
+        from . import engine
+        steps = self.steps if steps is None else int(steps)
+        t = self.tissue
+        with engine.Engine(self.dt, precision=precision, device=device) as e:
+            rid = [e.add_reaction(p) for p in self.params]
+            tid = e.add_tissue(t, np.asarray(rid, np.uint8)[self.reaction_of_cell])
+            if self.states is not None:
+                for k in range(tt06.NSTATE):
+                    e.write_state(tid, k, self.states[k])
+            rows = []
+            pos = int(np.searchsorted(t.gid, self.print_gid)) if self.print_rate else None
+            done = 0
+            while done < steps:
+                k = steps - done
+                if self.print_rate:
+                    k = min(k, self.print_rate - done % self.print_rate)
+                e.step(k)
+                done += k
+                if self.print_rate and done % self.print_rate == 0:
+                    s, time = e.time(tid)
+                    rows.append((s, time, self.print_gid, e.read_vm(tid)[pos]))
+            e.sync()
+            out = {"vm": e.read_vm(tid), "steps": done, "time": e.time(tid)[1], "print": np.array(rows)}
+            if "activationTime" in self.sensors:
+                out["activation"] = e.read_activation(tid)
+            if "minMax" in self.sensors:
+                out["minmax"] = e.minmax(tid)
+            return out
+
+
+def _brick(obj):
+    dx = objectdb.get_float(obj, "dx", 0.2)
+    dy = objectdb.get_float(obj, "dy", 0.2)
+    dz = objectdb.get_float(obj, "dz", 0.2)
+    if any(k in obj for k in ("nx", "ny", "nz")):
+        nx = int(objectdb.get_float(obj, "nx", 16))
+        ny = int(objectdb.get_float(obj, "ny", 16))
+        nz = int(objectdb.get_float(obj, "nz", 14))
+    else:
+        nx = int(objectdb.get_float(obj, "xSize", 3) / dx)
+        ny = int(objectdb.get_float(obj, "ySize", 7) / dy)
+        nz = int(objectdb.get_float(obj, "zSize", 20) / dz)
+    cell = objectdb.get_str(obj, "cellType", "102")
+    if cell == "random":
+        raise ValueError("ANATOMY brick with cellType = random is not supported")
+    n = nx * ny * nz
+    return (nx, ny, nz), (dx, dy, dz), np.arange(n, dtype=np.int64), np.full(n, int(cell), np.int32)
+
+
+def _uniform_sigma(obj, n):
+    g = lambda k: objectdb.get_float(obj, k, 0.0)
+    row = [g("sigma11"), g("sigma12"), g("sigma13"), g("sigma22"), g("sigma23"), g("sigma33")]
+    return np.tile(np.array(row, dtype=np.float64), (n, 1))
+
+
+def _stimulus(db, name, t):
+    obj = db.find(name, "STIMULUS")
+    method = objectdb.get_str(obj, "method", "undefined")
+    pulse = objectdb.get_str(obj, "pulse", "periodic")
+    if pulse != "periodic":
+        raise ValueError("STIMULUS %s: pulse %s is not supported (periodic only)" % (name, pulse))
+    g = lambda k, d: objectdb.get_float(obj, k, d)
+    kw = dict(vStim=g("vStim", -52.0), tStart=g("tStart", 0.0), duration=g("duration", 1.0),
+              period=g("period", 1000.0), t0=g("t0", -1000.0), tf=g("tf", 1e30))
+    if method == "box":
+        return tissue.BoxStim(xMin=g("xMin", -1), xMax=g("xMax", t.nx), yMin=g("yMin", -1), yMax=g("yMax", t.ny),
+                              zMin=g("zMin", -1), zMax=g("zMax", t.nz), **kw)
+    if method == "point":
+        cell = int(g("cell", 0))
+        return tissue.point_stim(int(t.gid[cell]), t.nx, t.ny, **kw)
+    raise ValueError("STIMULUS %s: method %s is not supported (box, point)" % (name, method))
+
+
+def load(paths, simulate=None, generate=None):
+    """Compiles the deck files (in order, as the reference's object files)
+    and builds the Simulation of the SIMULATE object `simulate` (the first
+    one when not named).  A pio anatomy's file name is taken relative to the
+    first deck file's directory."""
+    paths = [paths] if isinstance(paths, str) else list(paths)
+    db = objectdb.ObjectDB()
+    for p in paths:
+        db.compile_file(p)
+    base = os.path.dirname(os.path.abspath(paths[0]))
+    names = db.names("SIMULATE")
+    if not names:
+        raise ValueError("no SIMULATE object in the deck")
+    sim = db.find(simulate or names[0], "SIMULATE")
+    dt = objectdb.get_float(sim, "dt", 0.01)
+    steps = int(objectdb.get_float(sim, "maxLoop", 0)) - int(objectdb.get_float(sim, "loop", 0))
+
+    an = db.find(objectdb.get_str(sim, "anatomy", "anatomy"), "ANATOMY")
+    amethod = objectdb.get_str(an, "method", "pio")
+    cname = objectdb.get_str(an, "conductivity", "conductivity")
+    cond = db.find(cname, "CONDUCTIVITY") if db.exists(cname, "CONDUCTIVITY") else {}
+    cmethod = objectdb.get_str(cond, "method", "uniform") if cond else "pio"
+    if amethod == "brick":
+        grid, spacing, gid, ct = _brick(an)
+        if cmethod != "uniform":
+            raise ValueError("a brick anatomy takes a uniform CONDUCTIVITY")
+        sigma = _uniform_sigma(cond, len(gid))
+        t = tissue.Tissue(*grid, *spacing, gid, ct, sigma, np.full(len(gid), -83.0), [])
+    elif amethod == "pio":
+        fname = objectdb.get_str(an, "fileName", "snapshot.initial/anatomy#")
+        kw = dict(dx=objectdb.get_float(an, "dx", 0.2), dy=objectdb.get_float(an, "dy", 0.2),
+                  dz=objectdb.get_float(an, "dz", 0.2))
+        if cmethod == "fibre":
+            kw.update(conductivity="fibre", sigma_l=objectdb.get_float(cond, "sigmaLi", 0.3e-3),
+                      sigma_t=objectdb.get_float(cond, "sigmaTi", 0.0315e-3))
+        elif cmethod == "uniform":
+            kw.update(conductivity="uniform")
+        t = anatomy_mod.read_anatomy(os.path.join(base, fname), **kw)
+        if cmethod == "uniform":
+            t.sigma = _uniform_sigma(cond, t.n)
+    else:
+        raise ValueError("ANATOMY method %s is not supported (brick, pio)" % amethod)
+
+    dname = objectdb.get_str(sim, "diffusion", "diffusion")
+    dobj = db.find(dname, "DIFFUSION") if db.exists(dname, "DIFFUSION") else {}
+    dmethod = objectdb.get_str(dobj, "method", "FGR")
+    if dmethod == "null":
+        t.diffusion_scale = 0.0
+    elif dmethod in ("FGR", "b200"):
+        t.diffusion_scale = objectdb.get_float(dobj, "diffusionScale", 1.0)
+    else:
+        raise ValueError("DIFFUSION method %s: the fused engine runs FGR (use plugins.CUDADiffusion for cuda)"
+                         % dmethod)
+
+    rnames = objectdb.get_list(sim, "reaction")
+    params, type_of, vm_init, states = [], {}, [], []
+    have_states = False
+    for r, rn in enumerate(rnames):
+        robj = db.find(rn, "REACTION")
+        if objectdb.get_str(robj, "method", "") != "BetterTT06":
+            raise ValueError("REACTION %s: only BetterTT06 runs on the engine" % rn)
+        params.append(tt06.params_from_object(db, rn, dt, generate=generate))
+        for ct in objectdb.get_list(robj, "cellTypes"):
+            if int(ct) in type_of:
+                raise ValueError("duplicate cellTypes within the reaction models")
+            type_of[int(ct)] = r
+        v, st = tt06.initial_state_from_object(db, rn)
+        have_states = have_states or bool(st)
+        vm_init.append(v)
+        states.append(st)
+    missing = set(np.unique(t.cell_type).tolist()) - set(type_of)
+    if missing:
+        raise ValueError("no reaction for cellTypes %s" % sorted(missing))
+    rx = np.array([type_of[int(c)] for c in t.cell_type], dtype=np.uint8)
+    vm0 = np.array([v if v is not None else tt06.INITIAL_VM for v in vm_init])[rx]
+    t.vm0 = vm0
+    st_all = None
+    if have_states:
+        st_all = np.empty((tt06.NSTATE, t.n))
+        for r in range(len(params)):
+            sel = rx == r
+            for k, name in enumerate(tt06.STATE_NAMES):
+                st_all[k, sel] = states[r].get(name, tt06.INITIAL_STATE[name])
+
+    t.stimuli = [_stimulus(db, s, t) for s in objectdb.get_list(sim, "stimulus")]
+    sensors = [objectdb.get_str(db.find(s, "SENSOR"), "method", "") for s in objectdb.get_list(sim, "sensor")
+               if db.exists(s, "SENSOR")]
+    print_rate = int(objectdb.get_float(sim, "printRate", 0))
+    print_gid = int(objectdb.get_float(sim, "printGid", float(t.gid[0])))
+    return Simulation(t, params, rx, st_all, dt, steps, sensors, print_rate, print_gid)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description="Runs a Cardioid object.data deck on the B200 engine.")
+    ap.add_argument("files", nargs="+", help="object files, in the order the reference would read them")
+    ap.add_argument("--simulate", default=None, help="the SIMULATE object (default: the first)")
+    ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
+    ap.add_argument("--steps", type=int, default=None, help="steps to run (default: maxLoop - loop)")
+    ap.add_argument("--out", default=None, help="write Vm, activation times and printed rows to this .npz")
+    args = ap.parse_args(argv)
+    sim = load(args.files, args.simulate)
+    out = sim.run(args.precision, args.steps)
+    for row in out["print"]:
+        print("%12d %12.6f %12d %21.13e" % (int(row[0]), row[1], int(row[2]), row[3]))
+    if args.out:
+        np.savez(args.out, **{k: np.asarray(v) for k, v in out.items()})
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
