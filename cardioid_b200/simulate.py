@@ -11,7 +11,10 @@ omp time loop (elec/simulationLoop.cc:150-243) use it.
 What a deck may hold, per class (keys and defaults as the reference reads
 them):
   SIMULATE     anatomy, diffusion, reaction (list), stimulus (list), sensor
-               (list), dt, maxLoop, loop, time, printRate, printGid
+               (list), dt, maxLoop, loop, printRate, printGid,
+               checkpointRate, checkpointType (binary | ascii) and, as a
+               restart file merges them in, stateFile (loop and time from
+               its header)
   ANATOMY      method = brick (cellType, dx dy dz, xSize ySize zSize or nx
                ny nz; elec/initializeAnatomy.cc:147-239) or pio (fileName;
                cardioid_b200.anatomy.read_anatomy), conductivity
@@ -43,7 +46,12 @@ class Simulation:
     """A deck turned into engine inputs: tissue, reaction parameters and
     per-cell reaction ids, initial states, dt and step count."""
 
-    def __init__(self, t, params, reaction_of_cell, states, dt, steps, sensors, print_rate, print_gid):
+    def __init__(self, t, params, reaction_of_cell, states, dt, steps, sensors, print_rate, print_gid,
+                 checkpoint_rate=0, checkpoint_binary=True, state_file=None, name="simulate"):
+        self.checkpoint_rate = checkpoint_rate
+        self.checkpoint_binary = checkpoint_binary
+        self.state_file = state_file          # a restart's pio state file (loop and time from its header)
+        self.name = name
         self.tissue = t
         self.params = params
         self.reaction_of_cell = reaction_of_cell
@@ -54,11 +62,15 @@ class Simulation:
         self.print_rate = print_rate
         self.print_gid = print_gid
 
-    def run(self, precision="fp64", steps=None, device=0):
+    def run(self, precision="fp64", steps=None, device=0, out_dir="."):
         """Runs the deck's steps (or `steps`) on the fused engine and returns
         Vm, activation times, min/max Vm and the printed rows (loop, time,
-        gid, Vm every printRate steps, as the reference's printData)."""
-        from . import engine
+        gid, Vm whenever the loop count is a multiple of printRate, as the
+        reference's printData).  A restart (stateFile) starts from that
+        checkpoint's state, loop and time; with checkpointRate, checkpoints
+        go to out_dir/snapshot.<loop> at every multiple of it (the
+        reference's writeCheckpoint)."""
+        from . import checkpoint, engine
         steps = self.steps if steps is None else int(steps)
         t = self.tissue
         with engine.Engine(self.dt, precision=precision, device=device) as e:
@@ -67,20 +79,30 @@ class Simulation:
             if self.states is not None:
                 for k in range(tt06.NSTATE):
                     e.write_state(tid, k, self.states[k])
-            rows = []
+            if self.state_file:
+                checkpoint.restore(e, tid, t, self.state_file)
+            rows, saved = [], []
             pos = int(np.searchsorted(t.gid, self.print_gid)) if self.print_rate else None
+            loop0 = e.time(tid)[0]
             done = 0
             while done < steps:
+                loop = loop0 + done
                 k = steps - done
-                if self.print_rate:
-                    k = min(k, self.print_rate - done % self.print_rate)
+                for rate in (self.print_rate, self.checkpoint_rate):
+                    if rate:
+                        k = min(k, rate - loop % rate)
                 e.step(k)
                 done += k
-                if self.print_rate and done % self.print_rate == 0:
+                loop = loop0 + done
+                if self.print_rate and loop % self.print_rate == 0:
                     s, time = e.time(tid)
                     rows.append((s, time, self.print_gid, e.read_vm(tid)[pos]))
+                if self.checkpoint_rate and loop % self.checkpoint_rate == 0:
+                    saved.append(checkpoint.save(e, tid, t, binary=self.checkpoint_binary, name=self.name,
+                                                 root=out_dir))
             e.sync()
-            out = {"vm": e.read_vm(tid), "steps": done, "time": e.time(tid)[1], "print": np.array(rows)}
+            out = {"vm": e.read_vm(tid), "steps": done, "loop": e.time(tid)[0], "time": e.time(tid)[1],
+                   "print": np.array(rows), "checkpoints": saved}
             if "activationTime" in self.sensors:
                 out["activation"] = e.read_activation(tid)
             if "minMax" in self.sensors:
@@ -220,7 +242,13 @@ def load(paths, simulate=None, generate=None):
                if db.exists(s, "SENSOR")]
     print_rate = int(objectdb.get_float(sim, "printRate", 0))
     print_gid = int(objectdb.get_float(sim, "printGid", float(t.gid[0])))
-    return Simulation(t, params, rx, st_all, dt, steps, sensors, print_rate, print_gid)
+    state_file = objectdb.get_str(sim, "stateFile")
+    if state_file:
+        state_file = state_file if os.path.isabs(state_file) else os.path.join(base, state_file)
+    return Simulation(t, params, rx, st_all, dt, steps, sensors, print_rate, print_gid,
+                      checkpoint_rate=int(objectdb.get_float(sim, "checkpointRate", 0)),
+                      checkpoint_binary=objectdb.get_str(sim, "checkpointType", "binary") != "ascii",
+                      state_file=state_file, name=simulate or names[0])
 
 
 def main(argv=None):
@@ -230,13 +258,14 @@ def main(argv=None):
     ap.add_argument("--precision", choices=("fp64", "mixed"), default="fp64")
     ap.add_argument("--steps", type=int, default=None, help="steps to run (default: maxLoop - loop)")
     ap.add_argument("--out", default=None, help="write Vm, activation times and printed rows to this .npz")
+    ap.add_argument("--dir", default=".", help="where checkpoints go (checkpointRate)")
     args = ap.parse_args(argv)
     sim = load(args.files, args.simulate)
-    out = sim.run(args.precision, args.steps)
+    out = sim.run(args.precision, args.steps, out_dir=args.dir)
     for row in out["print"]:
         print("%12d %12.6f %12d %21.13e" % (int(row[0]), row[1], int(row[2]), row[3]))
     if args.out:
-        np.savez(args.out, **{k: np.asarray(v) for k, v in out.items()})
+        np.savez(args.out, **{k: np.asarray(v) for k, v in out.items() if k != "checkpoints"})
     return 0
 
 

@@ -104,3 +104,25 @@ def test_written_deck_runs_on_the_engine_as_the_oracle(cdb_lib, oracle_port, tmp
     np.testing.assert_array_equal(out["activation"], port.activation())
     assert (out["activation"] > 0).any()
     assert out["minmax"] == (out["vm"].min(), out["vm"].max())
+
+
+@pytest.mark.gpu
+def test_written_deck_checkpoints_and_restarts(cdb_lib, tmp_path):
+    """checkpointRate writes the reference's snapshot.<loop> directories; the
+    deck plus one of their restart files (merged into its SIMULATE object,
+    as the reference reads it) continues from that loop to the same Vm and
+    printed rows, bit for bit (binary checkpoints are exact)."""
+    files = _write_deck(tmp_path)
+    extra = tmp_path / "checkpoint.data"
+    extra.write_text("run SIMULATE { checkpointRate = 120; }")
+    full = simulate.load(files + [str(extra)]).run("fp64", out_dir=str(tmp_path))
+    assert [os.path.basename(d) for d in full["checkpoints"]] == ["snapshot.000000000120", "snapshot.000000000240"]
+    restart = os.path.join(str(tmp_path), "snapshot.000000000120", "restart")
+    again = simulate.load(files + [restart]).run("fp64", out_dir=str(tmp_path / "again"))
+    assert (again["loop"], again["steps"]) == (240, 120)
+    np.testing.assert_array_equal(again["vm"], full["vm"])
+    tail = full["print"][-len(again["print"]):]
+    np.testing.assert_array_equal(again["print"][:, [0, 2, 3]], tail[:, [0, 2, 3]])
+    # a restart takes its time from the checkpoint, as the reference's does:
+    # the accumulated time may differ in its last bits
+    np.testing.assert_allclose(again["print"][:, 1], tail[:, 1], rtol=0, atol=1e-12)
