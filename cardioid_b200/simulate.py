@@ -21,8 +21,9 @@ them):
   CONDUCTIVITY method = uniform (sigma11 sigma22 sigma33 sigma12 sigma13
                sigma23) or fibre (sigmaLi, sigmaTi: read with the pio
                anatomy's angles)
-  DIFFUSION    method = FGR (any variant) or b200, diffusionScale; method
-               null runs without diffusion
+  DIFFUSION    method = FGR (any variant) or b200 (the fused engine),
+               cuda (the 6-face rule: the split loop on the drop-in plugins),
+               null (no diffusion); diffusionScale
   REACTION     method = BetterTT06 (cardioid_b200.tt06.params_from_object),
                cellTypes; SINGLECELL objects named by a reaction set its
                cells' initial state
@@ -47,7 +48,9 @@ class Simulation:
     per-cell reaction ids, initial states, dt and step count."""
 
     def __init__(self, t, params, reaction_of_cell, states, dt, steps, sensors, print_rate, print_gid,
-                 checkpoint_rate=0, checkpoint_binary=True, state_file=None, name="simulate"):
+                 checkpoint_rate=0, checkpoint_binary=True, state_file=None, name="simulate",
+                 diffusion_method="FGR"):
+        self.diffusion_method = diffusion_method
         self.checkpoint_rate = checkpoint_rate
         self.checkpoint_binary = checkpoint_binary
         self.state_file = state_file          # a restart's pio state file (loop and time from its header)
@@ -73,6 +76,8 @@ class Simulation:
         from . import checkpoint, engine
         steps = self.steps if steps is None else int(steps)
         t = self.tissue
+        if self.diffusion_method == "cuda":
+            return self._run_split(precision, steps, device)
         with engine.Engine(self.dt, precision=precision, device=device) as e:
             rid = [e.add_reaction(p) for p in self.params]
             tid = e.add_tissue(t, np.asarray(rid, np.uint8)[self.reaction_of_cell])
@@ -108,6 +113,70 @@ class Simulation:
             if "minMax" in self.sensors:
                 out["minmax"] = e.minmax(tid)
             return out
+
+
+    def _run_split(self, precision, steps, device):
+        """The reference's omp loop on the drop-in plugins, for decks whose
+        DIFFUSION is the 6-face "cuda" rule (CUDADiffusion): iStim from the
+        stimuli in list order, one BetterTT06 plugin per reaction on its
+        cells, the 6-face diffusion, Vm += dt (dVmR + dVmD + iStim), time +=
+        dt, the activation rule after each step (elec/simulationLoop.cc:183-231)."""
+        import torch
+        from . import plugins
+        if self.state_file or self.checkpoint_rate:
+            raise ValueError("checkpoints and restarts run on the fused engine (FGR diffusion)")
+        t = self.tissue
+        dev = "cuda:%d" % device
+        vm = torch.from_numpy(np.ascontiguousarray(t.vm0, dtype=np.float64)).to(dev)
+        dvr, dvd, ist = torch.zeros_like(vm), torch.zeros_like(vm), torch.zeros_like(vm)
+        act = torch.full_like(vm, -1.0)
+        idx, rx = [], []
+        for r, p in enumerate(self.params):
+            cells = np.flatnonzero(self.reaction_of_cell == r).astype(np.int32)
+            idx.append(torch.from_numpy(cells).to(dev))
+            rx.append(plugins.BetterTT06(p, len(cells), self.dt, precision=precision, device=device))
+            if self.states is not None and len(cells):
+                for k in range(tt06.NSTATE):
+                    rx[-1].setValues(k, self.states[k][cells])
+        diff = plugins.CUDADiffusion(t, t.diffusion_scale, device=device) if t.diffusion_scale else None
+        x, y, z = t.tuples()
+        masks = []
+        for st in t.stimuli:
+            if st.mode == 1:
+                m = t.gid == st.cell
+            else:
+                m = (x > st.xMin) & (x < st.xMax) & (y > st.yMin) & (y < st.yMax) & (z > st.zMin) & (z < st.zMax)
+            masks.append(torch.from_numpy(m).to(dev))
+        pos = int(np.searchsorted(t.gid, self.print_gid)) if self.print_rate else None
+        rows, time = [], 0.0
+        for s in range(1, steps + 1):
+            ist.zero_()
+            for st, m in zip(t.stimuli, masks):
+                v = st.value(time)
+                if v != 0.0:
+                    if st.mode == 1:
+                        ist[m] += v
+                    else:
+                        ist[m] = v
+            for r in range(len(rx)):
+                if rx[r].nCells:
+                    rx[r].calc(self.dt, idx[r], vm, ist, dvr)
+            if diff is not None:
+                diff.updateLocalVoltage(vm)
+                diff.calc(dvd)
+            vm.add_(self.dt * (dvr + dvd + ist))
+            time += self.dt
+            act = torch.where((act < 0) & (vm > 0), torch.full_like(act, time), act)
+            if self.print_rate and s % self.print_rate == 0:
+                rows.append((s, time, self.print_gid, float(vm[pos])))
+        torch.cuda.synchronize(device)
+        v = vm.cpu().numpy()
+        out = {"vm": v, "steps": steps, "loop": steps, "time": time, "print": np.array(rows), "checkpoints": []}
+        if "activationTime" in self.sensors:
+            out["activation"] = act.cpu().numpy()
+        if "minMax" in self.sensors:
+            out["minmax"] = (float(v.min()), float(v.max()))
+        return out
 
 
 def _brick(obj):
@@ -201,11 +270,10 @@ def load(paths, simulate=None, generate=None):
     dmethod = objectdb.get_str(dobj, "method", "FGR")
     if dmethod == "null":
         t.diffusion_scale = 0.0
-    elif dmethod in ("FGR", "b200"):
+    elif dmethod in ("FGR", "b200", "cuda"):
         t.diffusion_scale = objectdb.get_float(dobj, "diffusionScale", 1.0)
     else:
-        raise ValueError("DIFFUSION method %s: the fused engine runs FGR (use plugins.CUDADiffusion for cuda)"
-                         % dmethod)
+        raise ValueError("DIFFUSION method %s is not supported (FGR, b200, cuda, null)" % dmethod)
 
     rnames = objectdb.get_list(sim, "reaction")
     params, type_of, vm_init, states = [], {}, [], []
@@ -248,7 +316,8 @@ def load(paths, simulate=None, generate=None):
     return Simulation(t, params, rx, st_all, dt, steps, sensors, print_rate, print_gid,
                       checkpoint_rate=int(objectdb.get_float(sim, "checkpointRate", 0)),
                       checkpoint_binary=objectdb.get_str(sim, "checkpointType", "binary") != "ascii",
-                      state_file=state_file, name=simulate or names[0])
+                      state_file=state_file, name=simulate or names[0],
+                      diffusion_method="cuda" if dmethod == "cuda" else "FGR")
 
 
 def main(argv=None):

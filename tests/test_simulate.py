@@ -126,3 +126,31 @@ def test_written_deck_checkpoints_and_restarts(cdb_lib, tmp_path):
     # a restart takes its time from the checkpoint, as the reference's does:
     # the accumulated time may differ in its last bits
     np.testing.assert_allclose(again["print"][:, 1], tail[:, 1], rtol=0, atol=1e-12)
+
+
+@pytest.mark.gpu
+def test_cuda_diffusion_deck_runs_the_split_loop_as_the_oracle(cdb_lib, oracle_port, tmp_path):
+    """A deck whose DIFFUSION is the 6-face "cuda" rule runs the split loop on
+    the drop-in plugins (BetterTT06 per reaction, CUDADiffusion); against the
+    oracle's reaction with the 6-face restatement added each step (same
+    inputs, 60 steps): Vm within 1e-6 mV (ulp-level differences grow to a few
+    1e-9 mV through the upstrokes), the same activation times."""
+    from oracle import diff6
+    files = _write_deck(tmp_path)
+    extra = tmp_path / "cuda.data"
+    extra.write_text("fgr DIFFUSION { method = cuda; }\nrun SIMULATE { maxLoop = 60; printRate = 0; }")
+    sim = simulate.load(files + [str(extra)])
+    assert sim.diffusion_method == "cuda"
+    out = sim.run("fp64")
+    t = sim.tissue
+    port = oracle_port.PortSim(t, sim.params, sim.reaction_of_cell, sim.dt, diffusion=False)
+    act = np.full(t.n, -1.0)
+    for _ in range(60):
+        v0 = port.vm()
+        d = diff6.calc(t, v0, t.diffusion_scale)
+        port.step(1)
+        v = port.vm() + sim.dt * d
+        port.set_vm(v)
+        act[(act < 0) & (v > 0)] = port.time
+    assert np.abs(out["vm"] - port.vm()).max() <= 1e-6      # the FP64 parity tolerance
+    np.testing.assert_array_equal(out["activation"], act)
