@@ -30,8 +30,10 @@ them):
   STIMULUS     method = box (xMin..zMax, elec/stimulusFactory.cc:96-110) or
                point (cell: a local cell index), pulse = periodic (vStim,
                tStart, duration, period, t0, tf)
-  SENSOR       method = activationTime or minMax: their results come back
-               from run()
+  SENSOR       method = activationTime (its times come back from run() and
+               go to out_dir/snapshot.<last loop>/<filename>#000000 in the
+               reference's record format; the engine evaluates every step)
+               or minMax
 Other methods raise ValueError (no silent substitution).
 """
 import argparse
@@ -51,6 +53,7 @@ class Simulation:
                  checkpoint_rate=0, checkpoint_binary=True, state_file=None, name="simulate",
                  diffusion_method="FGR"):
         self.diffusion_method = diffusion_method
+        self.activation_file = None           # the activationTime SENSOR's file name, written at the end
         self.checkpoint_rate = checkpoint_rate
         self.checkpoint_binary = checkpoint_binary
         self.state_file = state_file          # a restart's pio state file (loop and time from its header)
@@ -73,7 +76,7 @@ class Simulation:
         checkpoint's state, loop and time; with checkpointRate, checkpoints
         go to out_dir/snapshot.<loop> at every multiple of it (the
         reference's writeCheckpoint)."""
-        from . import checkpoint, engine
+        from . import checkpoint, engine, sensors
         steps = self.steps if steps is None else int(steps)
         t = self.tissue
         if self.diffusion_method == "cuda":
@@ -110,6 +113,11 @@ class Simulation:
                    "print": np.array(rows), "checkpoints": saved}
             if "activationTime" in self.sensors:
                 out["activation"] = e.read_activation(tid)
+                if self.activation_file:
+                    loop, time = e.time(tid)
+                    out["activation_file"] = sensors.write_activation(
+                        os.path.join(out_dir, "snapshot.%012d" % loop), t.gid, out["activation"], loop, time,
+                        (t.nx, t.ny, t.nz), (t.dx, t.dy, t.dz), filename=self.activation_file)
             if "minMax" in self.sensors:
                 out["minmax"] = e.minmax(tid)
             return out
@@ -306,18 +314,24 @@ def load(paths, simulate=None, generate=None):
                 st_all[k, sel] = states[r].get(name, tt06.INITIAL_STATE[name])
 
     t.stimuli = [_stimulus(db, s, t) for s in objectdb.get_list(sim, "stimulus")]
-    sensors = [objectdb.get_str(db.find(s, "SENSOR"), "method", "") for s in objectdb.get_list(sim, "sensor")
-               if db.exists(s, "SENSOR")]
+    sensor_objs = [db.find(s, "SENSOR") for s in objectdb.get_list(sim, "sensor") if db.exists(s, "SENSOR")]
+    sensors = [objectdb.get_str(o, "method", "") for o in sensor_objs]
+    act_file = None
+    for o in sensor_objs:
+        if objectdb.get_str(o, "method", "") == "activationTime":
+            act_file = objectdb.get_str(o, "filename", "activationTime")
     print_rate = int(objectdb.get_float(sim, "printRate", 0))
     print_gid = int(objectdb.get_float(sim, "printGid", float(t.gid[0])))
     state_file = objectdb.get_str(sim, "stateFile")
     if state_file:
         state_file = state_file if os.path.isabs(state_file) else os.path.join(base, state_file)
-    return Simulation(t, params, rx, st_all, dt, steps, sensors, print_rate, print_gid,
+    out = Simulation(t, params, rx, st_all, dt, steps, sensors, print_rate, print_gid,
                       checkpoint_rate=int(objectdb.get_float(sim, "checkpointRate", 0)),
                       checkpoint_binary=objectdb.get_str(sim, "checkpointType", "binary") != "ascii",
                       state_file=state_file, name=simulate or names[0],
                       diffusion_method="cuda" if dmethod == "cuda" else "FGR")
+    out.activation_file = act_file
+    return out
 
 
 def main(argv=None):

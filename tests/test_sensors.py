@@ -29,3 +29,20 @@ def test_apd90_ignores_an_unfinished_beat():
     t = np.arange(0.0, 300.0, 0.1)
     assert len(apd90(_beat(t, 100.0, 400.0), t)) == 0
     assert len(apd90(np.full_like(t, -85.0), t)) == 0
+
+
+def test_activation_file_reads_back(tmp_path):
+    """The activation-time file in the reference's record format (32-byte
+    ASCII records, gid and time to 12 decimals, 0 for cells that never
+    activated) reads back through the pio reader."""
+    from cardioid_b200 import pio, sensors
+    gid = np.array([0, 5, 2 ** 33 + 7], dtype=np.int64)
+    act = np.array([1.25, -1.0, 12.345678901234])
+    path = sensors.write_activation(str(tmp_path / "snapshot.000000000120"), gid, act, 120, 2.4, (10, 8, 6),
+                                    (0.2, 0.2, 0.2))
+    body = open(path).read().split("}\n\n", 1)[1]
+    assert [len(line) + 1 for line in body.splitlines()] == [32, 32, 32]
+    f = pio.read(path[:-len("#000000")])
+    np.testing.assert_array_equal(f.fields["gid"], gid)
+    np.testing.assert_allclose(f.fields["tActiv"], [1.25, 0.0, 12.345678901234], rtol=0, atol=1e-12)
+    assert int(f.header["loop"]) == 120

@@ -93,7 +93,7 @@ def test_written_deck_loads(tmp_path):
 @pytest.mark.gpu
 def test_written_deck_runs_on_the_engine_as_the_oracle(cdb_lib, oracle_port, tmp_path):
     sim = simulate.load(_write_deck(tmp_path))
-    out = sim.run("fp64")
+    out = sim.run("fp64", out_dir=str(tmp_path))
     port = oracle_port.PortSim(sim.tissue, sim.params, sim.reaction_of_cell, sim.dt)
     pos = int(np.searchsorted(sim.tissue.gid, sim.print_gid))
     for row in out["print"]:
@@ -102,6 +102,10 @@ def test_written_deck_runs_on_the_engine_as_the_oracle(cdb_lib, oracle_port, tmp
     assert out["steps"] == 240 and abs(out["time"] - port.time) < 1e-12
     assert np.abs(out["vm"] - port.vm()).max() <= 1e-6
     np.testing.assert_array_equal(out["activation"], port.activation())
+    from cardioid_b200 import pio
+    f = pio.read(out["activation_file"][:-len("#000000")])
+    np.testing.assert_array_equal(f.fields["gid"], sim.tissue.gid)
+    np.testing.assert_allclose(f.fields["tActiv"], np.maximum(out["activation"], 0.0), rtol=0, atol=1e-12)
     assert (out["activation"] > 0).any()
     assert out["minmax"] == (out["vm"].min(), out["vm"].max())
 
