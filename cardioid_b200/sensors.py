@@ -62,3 +62,15 @@ def write_activation(directory, gid, activation, loop, time, grid, spacing, file
     with open(path, "w") as f:
         f.write(header + rows)
     return path
+
+
+def write_minmax(path, rows):
+    """Writes the rows (time, min Vm, max Vm) as MinMaxSensor::print does
+    (elec/MinMaxSensor.cc:30-68): a header line, then time, min, max and
+    max - min in scientific notation with 10 digits.  Returns the path."""
+    os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+    with open(path, "w") as f:
+        f.write("#    time   min V_m    max V_m    max-min\n")
+        for time, lo, hi in rows:
+            f.write(" %.10e     %.10e      %.10e    %.10e\n" % (time, lo, hi, hi - lo))
+    return path

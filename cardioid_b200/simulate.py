@@ -33,7 +33,8 @@ them):
   SENSOR       method = activationTime (its times come back from run() and
                go to out_dir/snapshot.<last loop>/<filename>#000000 in the
                reference's record format; the engine evaluates every step)
-               or minMax
+               or minMax (time, min, max, max - min every printRate steps
+               to out_dir/dirname/filename, as MinMaxSensor::print)
 Other methods raise ValueError (no silent substitution).
 """
 import argparse
@@ -54,6 +55,7 @@ class Simulation:
                  diffusion_method="FGR"):
         self.diffusion_method = diffusion_method
         self.activation_file = None           # the activationTime SENSOR's file name, written at the end
+        self.minmax_out = None                # the minMax SENSOR's (printRate, dirname/filename)
         self.checkpoint_rate = checkpoint_rate
         self.checkpoint_binary = checkpoint_binary
         self.state_file = state_file          # a restart's pio state file (loop and time from its header)
@@ -80,7 +82,7 @@ class Simulation:
         steps = self.steps if steps is None else int(steps)
         t = self.tissue
         if self.diffusion_method == "cuda":
-            return self._run_split(precision, steps, device)
+            return self._run_split(precision, steps, device, out_dir)
         with engine.Engine(self.dt, precision=precision, device=device) as e:
             rid = [e.add_reaction(p) for p in self.params]
             tid = e.add_tissue(t, np.asarray(rid, np.uint8)[self.reaction_of_cell])
@@ -89,14 +91,15 @@ class Simulation:
                     e.write_state(tid, k, self.states[k])
             if self.state_file:
                 checkpoint.restore(e, tid, t, self.state_file)
-            rows, saved = [], []
+            rows, saved, mm_rows = [], [], []
             pos = int(np.searchsorted(t.gid, self.print_gid)) if self.print_rate else None
             loop0 = e.time(tid)[0]
             done = 0
             while done < steps:
                 loop = loop0 + done
                 k = steps - done
-                for rate in (self.print_rate, self.checkpoint_rate):
+                mm_rate = self.minmax_out[0] if self.minmax_out else 0
+                for rate in (self.print_rate, self.checkpoint_rate, mm_rate):
                     if rate:
                         k = min(k, rate - loop % rate)
                 e.step(k)
@@ -105,6 +108,9 @@ class Simulation:
                 if self.print_rate and loop % self.print_rate == 0:
                     s, time = e.time(tid)
                     rows.append((s, time, self.print_gid, e.read_vm(tid)[pos]))
+                if mm_rate and loop % mm_rate == 0:
+                    lo, hi = e.minmax(tid)
+                    mm_rows.append((e.time(tid)[1], lo, hi))
                 if self.checkpoint_rate and loop % self.checkpoint_rate == 0:
                     saved.append(checkpoint.save(e, tid, t, binary=self.checkpoint_binary, name=self.name,
                                                  root=out_dir))
@@ -120,17 +126,19 @@ class Simulation:
                         (t.nx, t.ny, t.nz), (t.dx, t.dy, t.dz), filename=self.activation_file)
             if "minMax" in self.sensors:
                 out["minmax"] = e.minmax(tid)
+                if self.minmax_out:
+                    out["minmax_file"] = sensors.write_minmax(os.path.join(out_dir, self.minmax_out[1]), mm_rows)
             return out
 
 
-    def _run_split(self, precision, steps, device):
+    def _run_split(self, precision, steps, device, out_dir="."):
         """The reference's omp loop on the drop-in plugins, for decks whose
         DIFFUSION is the 6-face "cuda" rule (CUDADiffusion): iStim from the
         stimuli in list order, one BetterTT06 plugin per reaction on its
         cells, the 6-face diffusion, Vm += dt (dVmR + dVmD + iStim), time +=
         dt, the activation rule after each step (elec/simulationLoop.cc:183-231)."""
         import torch
-        from . import plugins
+        from . import plugins, sensors
         if self.state_file or self.checkpoint_rate:
             raise ValueError("checkpoints and restarts run on the fused engine (FGR diffusion)")
         t = self.tissue
@@ -156,7 +164,8 @@ class Simulation:
                 m = (x > st.xMin) & (x < st.xMax) & (y > st.yMin) & (y < st.yMax) & (z > st.zMin) & (z < st.zMax)
             masks.append(torch.from_numpy(m).to(dev))
         pos = int(np.searchsorted(t.gid, self.print_gid)) if self.print_rate else None
-        rows, time = [], 0.0
+        rows, mm_rows, time = [], [], 0.0
+        mm_rate = self.minmax_out[0] if self.minmax_out else 0
         for s in range(1, steps + 1):
             ist.zero_()
             for st, m in zip(t.stimuli, masks):
@@ -177,13 +186,21 @@ class Simulation:
             act = torch.where((act < 0) & (vm > 0), torch.full_like(act, time), act)
             if self.print_rate and s % self.print_rate == 0:
                 rows.append((s, time, self.print_gid, float(vm[pos])))
+            if mm_rate and s % mm_rate == 0:
+                mm_rows.append((time, float(vm.min()), float(vm.max())))
         torch.cuda.synchronize(device)
         v = vm.cpu().numpy()
         out = {"vm": v, "steps": steps, "loop": steps, "time": time, "print": np.array(rows), "checkpoints": []}
         if "activationTime" in self.sensors:
             out["activation"] = act.cpu().numpy()
+            if self.activation_file:
+                out["activation_file"] = sensors.write_activation(
+                    os.path.join(out_dir, "snapshot.%012d" % steps), t.gid, out["activation"], steps, time,
+                    (t.nx, t.ny, t.nz), (t.dx, t.dy, t.dz), filename=self.activation_file)
         if "minMax" in self.sensors:
             out["minmax"] = (float(v.min()), float(v.max()))
+            if self.minmax_out:
+                out["minmax_file"] = sensors.write_minmax(os.path.join(out_dir, self.minmax_out[1]), mm_rows)
         return out
 
 
@@ -316,10 +333,14 @@ def load(paths, simulate=None, generate=None):
     t.stimuli = [_stimulus(db, s, t) for s in objectdb.get_list(sim, "stimulus")]
     sensor_objs = [db.find(s, "SENSOR") for s in objectdb.get_list(sim, "sensor") if db.exists(s, "SENSOR")]
     sensors = [objectdb.get_str(o, "method", "") for o in sensor_objs]
-    act_file = None
+    act_file, minmax_out = None, None
     for o in sensor_objs:
         if objectdb.get_str(o, "method", "") == "activationTime":
             act_file = objectdb.get_str(o, "filename", "activationTime")
+        if objectdb.get_str(o, "method", "") == "minMax":
+            minmax_out = (int(objectdb.get_float(o, "printRate", 1)),
+                          os.path.join(objectdb.get_str(o, "dirname", "sensorData"),
+                                       objectdb.get_str(o, "filename", "minmax")))
     print_rate = int(objectdb.get_float(sim, "printRate", 0))
     print_gid = int(objectdb.get_float(sim, "printGid", float(t.gid[0])))
     state_file = objectdb.get_str(sim, "stateFile")
@@ -331,6 +352,7 @@ def load(paths, simulate=None, generate=None):
                       state_file=state_file, name=simulate or names[0],
                       diffusion_method="cuda" if dmethod == "cuda" else "FGR")
     out.activation_file = act_file
+    out.minmax_out = minmax_out
     return out
 
 

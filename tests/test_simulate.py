@@ -72,7 +72,7 @@ mid REACTION { method = BetterTT06; cellTypes = 101; celltype = 1; %s }
 s1 STIMULUS { method = box; xMax = 2; vStim = -52; duration = 1; period = 1000; }
 pt STIMULUS { method = point; cell = 500; vStim = -30; tStart = 2; duration = 0.5; }
 act SENSOR { method = activationTime; }
-mm SENSOR { method = minMax; }
+mm SENSOR { method = minMax; printRate = 60; }
 """ % (dt, ("fit = %s;" % fit_name) if fit_name else "")
     path = tmp_path / "object.data"
     path.write_text(deck)
@@ -108,6 +108,9 @@ def test_written_deck_runs_on_the_engine_as_the_oracle(cdb_lib, oracle_port, tmp
     np.testing.assert_allclose(f.fields["tActiv"], np.maximum(out["activation"], 0.0), rtol=0, atol=1e-12)
     assert (out["activation"] > 0).any()
     assert out["minmax"] == (out["vm"].min(), out["vm"].max())
+    mm = np.loadtxt(out["minmax_file"])          # time, min, max, max - min every 60 steps
+    assert mm.shape == (4, 4)
+    np.testing.assert_allclose(mm[-1, 1:3], [out["vm"].min(), out["vm"].max()], rtol=1e-9)
 
 
 @pytest.mark.gpu
@@ -145,7 +148,8 @@ def test_cuda_diffusion_deck_runs_the_split_loop_as_the_oracle(cdb_lib, oracle_p
     extra.write_text("fgr DIFFUSION { method = cuda; }\nrun SIMULATE { maxLoop = 60; printRate = 0; }")
     sim = simulate.load(files + [str(extra)])
     assert sim.diffusion_method == "cuda"
-    out = sim.run("fp64")
+    out = sim.run("fp64", out_dir=str(tmp_path / "cuda"))
+    assert np.loadtxt(out["minmax_file"], ndmin=2).shape == (1, 4)     # printRate 60 over 60 steps
     t = sim.tissue
     port = oracle_port.PortSim(t, sim.params, sim.reaction_of_cell, sim.dt, diffusion=False)
     act = np.full(t.n, -1.0)
