@@ -15,6 +15,19 @@ def test_library_exports_every_declared_symbol(cdb_lib):
     assert not missing, missing
 
 
+def test_checked_library_exports_the_same_symbols(cdb_lib):
+    """The bounds-checked build (libcardioid_b200_checked.so, built beside
+    the library) is a drop-in for it: every declared symbol is exported."""
+    import os
+    import pytest
+    from cardioid_b200 import build
+    if not os.path.exists(build.CHECKED_LIB):
+        pytest.skip("checked library not built")
+    lib = ctypes.CDLL(build.CHECKED_LIB)
+    missing = [s for s in _lib.declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
 def test_version_and_error_strings(cdb_lib):
     assert b"sm_100a" in cdb_lib.cdb_version()
     assert isinstance(cdb_lib.cdb_last_error(), bytes)
