@@ -162,3 +162,21 @@ def test_cuda_diffusion_deck_runs_the_split_loop_as_the_oracle(cdb_lib, oracle_p
         act[(act < 0) & (v > 0)] = port.time
     assert np.abs(out["vm"] - port.vm()).max() <= 1e-6      # the FP64 parity tolerance
     np.testing.assert_array_equal(out["activation"], act)
+
+
+@pytest.mark.parametrize("patch,match", [
+    ("slab ANATOMY { method = simple; }", "ANATOMY method simple"),
+    ("fgr DIFFUSION { method = gpu; }", "DIFFUSION method gpu"),
+    ("s1 STIMULUS { method = test; }", "method test"),
+    ("s1 STIMULUS { pulse = random; }", "pulse random"),
+    ("mid REACTION { method = TT06Dev; }", "only BetterTT06"),
+    ("slab ANATOMY { cellType = 102; }", "no reaction for cellTypes"),
+])
+def test_unsupported_deck_items_raise(tmp_path, patch, match):
+    """What the engine does not run is refused with ValueError, never
+    replaced by something else."""
+    files = _write_deck(tmp_path)
+    extra = tmp_path / "patch.data"
+    extra.write_text(patch)
+    with pytest.raises(ValueError, match=match):
+        simulate.load(files + [str(extra)])
