@@ -7,7 +7,23 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-REFERENCE = "/root/reference"
+
+
+def reference_root():
+    """The reference (Cardioid) checkout whose golden files the pins read:
+    CARDIOID_REF, else where the oracle build found it
+    (oracle/_ref/reference_root, written by oracle/ref/Makefile); an empty
+    string when neither names an existing directory (the pins then skip)."""
+    cand = os.environ.get("CARDIOID_REF", "")
+    if not cand:
+        rec = os.path.join(ROOT, "oracle", "_ref", "reference_root")
+        if os.path.exists(rec):
+            with open(rec) as f:
+                cand = f.read().strip()
+    return cand if cand and os.path.isdir(cand) else ""
+
+
+REFERENCE = reference_root()
 
 
 def pytest_configure(config):

@@ -9,6 +9,7 @@ The inputs go through this package's own readers (pio anatomy, object
 database, fit reuse rule, initial-state rule), so the fixture is the
 reference's data as the engine sees it.  Run from the repository root:
     python tests/golden/make_multiple_reaction.py [reference checkout]
+(default: CARDIOID_REF, else the checkout the oracle build recorded).
 """
 import os
 import sys
@@ -62,4 +63,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    sys.path.insert(0, os.path.join(HERE, ".."))
+    from conftest import reference_root
+    main(sys.argv[1] if len(sys.argv) > 1 else reference_root())

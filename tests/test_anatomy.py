@@ -13,9 +13,10 @@ import numpy as np
 import pytest
 
 from cardioid_b200 import anatomy, tissue, tt06
+from conftest import REFERENCE
 
 FIX = os.path.join(os.path.dirname(__file__), "golden", "multiple_reaction.npz")
-REF_ANATOMY = "/root/reference/test/tests/multipleReaction/snapshot.initial/anatomy#"
+REF_ANATOMY = os.path.join(REFERENCE, "test", "tests", "multipleReaction", "snapshot.initial", "anatomy#")
 # The reference compares these traces to 1e-14 on its own platform; the
 # oracle (glibc libm) lands 9e-6 mV from them after 30 000 steps, the spread
 # of one-ulp differences in exp/log through the upstrokes.
@@ -41,7 +42,7 @@ def case():
     return t, params, rx, states, float(d["dt"]), int(d["steps"]), pos, d["traces"]
 
 
-@pytest.mark.skipif(not os.path.exists(REF_ANATOMY + "000000"), reason="needs the reference checkout")
+@pytest.mark.skipif(not (REFERENCE and os.path.exists(REF_ANATOMY + "000000")), reason="needs the reference checkout")
 def test_anatomy_reader_matches_fixture():
     t = anatomy.read_anatomy(REF_ANATOMY)
     d = np.load(FIX)

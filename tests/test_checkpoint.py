@@ -10,8 +10,9 @@ import numpy as np
 import pytest
 
 from cardioid_b200 import checkpoint, tt06
+from conftest import REFERENCE
 
-REF_FIXTURE = "/root/reference/test/tests/diffusionTest/snapshot.000000000001/state#"
+REF_FIXTURE = os.path.join(REFERENCE, "test", "tests", "diffusionTest", "snapshot.000000000001", "state#")
 
 
 def _ref_built():
@@ -71,7 +72,7 @@ def test_reference_reader_reads_our_checkpoint(tmp_path, binary):
         np.testing.assert_array_equal(vals[:, 1], vm)
 
 
-@pytest.mark.skipif(not (_ref_built() and os.path.exists(REF_FIXTURE + "000000")),
+@pytest.mark.skipif(not (_ref_built() and REFERENCE and os.path.exists(REF_FIXTURE + "000000")),
                     reason="needs the reference checkout and oracle/_ref")
 def test_reference_fixture_reads_the_same_in_both_readers():
     from oracle import refsim

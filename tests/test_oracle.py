@@ -10,7 +10,7 @@ import pytest
 from conftest import REFERENCE
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-HAVE_REF_TREE = os.path.exists(os.path.join(REFERENCE, "test", "tests"))
+HAVE_REF_TREE = bool(REFERENCE) and os.path.exists(os.path.join(REFERENCE, "test", "tests"))
 
 
 def _ref_built():

@@ -18,7 +18,7 @@ from cardioid_b200 import engine, simulate, tissue
 from conftest import REFERENCE
 
 TESTS = os.path.join(REFERENCE, "test", "tests")
-HAVE_DECKS = os.path.exists(os.path.join(TESTS, "Niederer", "object.data"))
+HAVE_DECKS = bool(REFERENCE) and os.path.exists(os.path.join(TESTS, "Niederer", "object.data"))
 
 
 @pytest.mark.skipif(not HAVE_DECKS, reason="reference checkout not present")
