@@ -143,12 +143,20 @@ def transmural_types(x, nx, endo_frac=0.25, mid_frac=0.35):
 
 
 def box(nx, ny, nz, dx=0.2, seed=20240611, period=1000.0, duration=1.0, vstim=-52.0,
-        angle_min_deg=-60.0, angle_max_deg=60.0, stim_face=True):
+        angle_min_deg=-60.0, angle_max_deg=60.0, stim_face=True, zrange=None):
     """A dense box of tissue, the workload of the reference's Niederer-style
     runs restated on our conventions (cell types by x-slab, fibre angle
-    rotating linearly across z, a pacing stimulus on the x = 0 face)."""
-    n = nx * ny * nz
-    gid = np.arange(n, dtype=np.int64)
+    rotating linearly across z, a pacing stimulus on the x = 0 face).
+
+    zrange = (z0, z1) keeps only the cells with z0 <= z < z1 (one rank's
+    slab of the box, as a z-decomposition over processes gives it): the same
+    gids, fibres, types, initial Vm and stimulus as in the whole box; the
+    slab's faces at z0 and z1 - 1 have no neighbours (no-flux)."""
+    z0, z1 = zrange if zrange is not None else (0, nz)
+    if not (0 <= z0 < z1 <= nz):
+        raise ValueError("zrange outside the box")
+    gid = np.arange(z0 * nx * ny, z1 * nx * ny, dtype=np.int64)
+    n = gid.shape[0]
     x = gid % nx
     z = gid // (nx * ny)
     ct = transmural_types(x, nx)
