@@ -31,7 +31,6 @@ METRIC = "cell-steps/s"
 # stencil weights FP64 19x8 = 152 B, mixed 18x4 = 72 B; the cell's voxel
 # offset 4 B (the reaction type is per warp tile, not per cell).
 ALGO_BYTES = {"fp64": 16 + 288 + 152 + 4, "mixed": 16 + 184 + 72 + 4}
-CPU_SAMPLE = (64, 64, 32)     # cells per CPU worker process
 
 
 def workload(name):
@@ -39,6 +38,9 @@ def workload(name):
         return dict(nx=256, ny=256, nz=256, period=500.0, label="box256: 256^3 = 16,777,216 cells, dx 0.2 mm, "
                     "endo/mid/epi x-slabs 25/35/40 %, fibre -60..+60 deg across z, sigma_l 0.133 / sigma_t 0.0176 S/m, "
                     "beta 1400/cm, Cm 1 uF/cm^2, S1 pacing every 500 ms on the x = 0 face, dt 0.02 ms")
+    if name == "box192":
+        return dict(nx=192, ny=192, nz=192, period=500.0, label="box192: 192^3 = 7,077,888 cells (traffic capture "
+                    "size: every launch writes far more than L2), otherwise as box256")
     if name == "box128":
         return dict(nx=128, ny=128, nz=128, period=500.0, label="box128: 128^3 = 2,097,152 cells (profiling size), "
                     "otherwise as box256")
@@ -46,6 +48,15 @@ def workload(name):
         return dict(nx=64, ny=64, nz=64, period=1000.0, label="box64: 64^3 = 262,144 cells, single stimulus at t = 0 "
                     "on the x = 0 face, otherwise as box256")
     raise ValueError(name)
+
+
+def bench_config(w, world):
+    """The `config` object of both arms' lines (same workload, same keys)."""
+    n = w["nx"] * w["ny"] * w["nz"]
+    return {"workload": w["label"], "cells_per_gpu": n, "dt_ms": DT,
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (state + weights %.1f GB per GPU, mixed)" % (
+                (ALGO_BYTES["mixed"] - 16) * n / 1e9)}
 
 
 def read_peaks():
@@ -72,16 +83,16 @@ def read_traffic(precision):
 # ---------------------------------------------------------------- CPU side
 
 def _cpu_worker(args):
-    """Runs the reference CPU path (oracle/_ref) or the oracle port on one
-    sample box with `threads` OpenMP threads (the reference's omp loop: the
-    FGR stencil threaded, BetterTT06 single-threaded); returns (cells,
-    steps, seconds)."""
-    kind, shape, steps, warmup, seed = args[:5]
-    threads = args[5] if len(args) > 5 else 1
+    """Runs the reference CPU path (oracle/_ref) or the oracle port on the
+    workload's box, or on one z-slab of it, with `threads` OpenMP threads
+    (the reference's omp loop: the FGR stencil threaded, BetterTT06
+    single-threaded); returns (cells, steps, seconds, set-up seconds)."""
+    kind, box, zrange, steps, warmup, threads = args
     os.environ["OMP_NUM_THREADS"] = str(threads)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from cardioid_b200 import engine, tissue
-    t = tissue.box(*shape, seed=seed)
+    s0 = time.perf_counter()
+    t = tissue.box(box["nx"], box["ny"], box["nz"], period=box["period"], seed=1234, zrange=zrange)
     if kind == "reference":
         from golden.make_golden import reference_sim
         from oracle import refsim
@@ -92,48 +103,78 @@ def _cpu_worker(args):
         from oracle import port
         params = [engine.default_params(ct, DT) for ct in (0, 1, 2)]
         sim = port.PortSim(t, params, (t.cell_type - 100).astype(np.uint8), DT)
+    setup = time.perf_counter() - s0
     sim.step(warmup)
     t0 = time.perf_counter()
     sim.step(steps)
-    return t.n, steps, time.perf_counter() - t0
+    return t.n, steps, time.perf_counter() - t0, setup
 
 
-def cpu_baseline(steps, warmup, procs=None):
-    from oracle import refsim
-    kind = "reference" if refsim.available() else "port"
-    procs = procs or os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(procs) as pool:
-        res = pool.map(_cpu_worker, [(kind, CPU_SAMPLE, steps, warmup, 100 + i) for i in range(procs)])
-    cells = sum(r[0] * r[1] for r in res)
-    wall = max(r[2] for r in res)
-    cpu = ""
+def _cpu_model():
     try:
         with open("/proc/cpuinfo") as f:
             for line in f:
                 if line.startswith("model name"):
-                    cpu = line.split(":", 1)[1].strip()
-                    break
+                    return line.split(":", 1)[1].strip()
     except OSError:
         pass
-    what = ("the reference's own CPU path (oracle/_ref: BetterTT06 + FGRDiffusionOMP + BoxStimulus, omp-loop order)"
-            if kind == "reference" else "the oracle's C restatement of the reference path")
+    return ""
+
+
+def cpu_baseline(box, steps, warmup, omp_steps=2, procs=None):
+    """The reference's CPU path on the workload's own geometry.
+
+    value: one single-threaded process per host core, each stepping one
+    z-slab of the box (the decomposition the reference gives its MPI ranks,
+    here without the halo exchange: slab faces are no-flux), `steps` steps
+    after `warmup`; the rate is all cells x steps / the slowest process.
+    omp_loop_one_process: the whole box in one process, the reference's omp
+    loop as shipped (stencil on every core, reaction on one), `omp_steps`
+    steps after one warm-up step."""
+    from oracle import refsim
+    kind = "reference" if refsim.available() else "port"
+    procs = procs or os.cpu_count() or 1
+    nz = box["nz"]
+    cuts = [round(nz * r / procs) for r in range(procs + 1)]
+    jobs = [(kind, box, (cuts[r], cuts[r + 1]), steps, warmup, 1) for r in range(procs) if cuts[r + 1] > cuts[r]]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(len(jobs)) as pool:
+        res = pool.map(_cpu_worker, jobs)
+    cells = sum(r[0] for r in res)
+    wall = max(r[2] for r in res)
     per_core = sum(r[0] * r[1] / r[2] for r in res) / len(res)
-    # the reference as it runs: one process, the stencil on every core
-    with ctx.Pool(1) as pool:
-        n1, s1, w1 = pool.map(_cpu_worker, [(kind, CPU_SAMPLE, steps, warmup, 100, procs)])[0]
-    return {"value": cells / wall, "unit": METRIC, "cores": procs, "kind": kind, "per_core": per_core,
-            "omp_loop_one_process": n1 * s1 / w1,
-            "sample": "%s; %d processes (one per host core, like one MPI rank per core, no halo exchange), "
-                      "each a %dx%dx%d box of the same workload for %d steps after %d warm-up; "
-                      "omp_loop_one_process: one process on the same box with the stencil's OpenMP loop on every "
-                      "core and the reaction on one, as the reference's omp loop runs; CPU: %s"
-                      % (what, procs, CPU_SAMPLE[0], CPU_SAMPLE[1], CPU_SAMPLE[2], steps, warmup, cpu)}
+    out = {"value": cells * steps / wall, "unit": METRIC, "cores": procs, "kind": kind, "per_core": per_core,
+           "cells": cells, "steps": steps}
+    what = ("the reference's own CPU path (oracle/_ref: BetterTT06 via ReactionManager + FGRDiffusionOMP + "
+            "BoxStimulus, omp-loop order)" if kind == "reference" else "the oracle's C restatement of the reference path")
+    omp = None
+    if omp_steps > 0:
+        with ctx.Pool(1) as pool:
+            n1, s1, w1, su1 = pool.map(_cpu_worker, [(kind, box, None, omp_steps, 1, procs)])[0]
+        omp = n1 * s1 / w1
+        out["omp_loop_one_process"] = omp
+        out["omp_loop_setup_s"] = su1
+    out["sample"] = (
+        "%s on the %dx%dx%d box (%d cells): %d processes, one per host core, each a z-slab of the box (the "
+        "reference's MPI-style decomposition, no halo exchange), %d steps after %d warm-up; omp_loop_one_process: "
+        "the whole box in one process, stencil on %d OpenMP threads and the reaction on one as the reference's omp "
+        "loop runs, %d steps after 1 warm-up; CPU: %s" % (what, box["nx"], box["ny"], nz, cells, len(jobs), steps,
+                                                          warmup, procs, omp_steps, _cpu_model()))
+    return out
 
 
 # ---------------------------------------------------------------- clocks
 
 class ClockSampler:
+    """SM clock and clock-event reasons of one GPU during a timed region.
+
+    The caller polls: `sample()` reads the current SM clock and the active
+    clock-event reasons through NVML (well under a millisecond per call), so
+    a timed region of a few milliseconds still gets samples.  Without NVML
+    it falls back to `nvidia-smi -lms 200` in the background (long regions
+    only)."""
+    NVML_REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+                    ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -142,8 +183,30 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines = []
+        self.nvml = None
+        self.sm, self.reasons, self.max_mhz = [], set(), None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.device)
+            bus = "%08X:%02X:%02X.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+        return pynvml, h
 
     def __enter__(self):
+        try:
+            self.nvml = self._nvml_handle()
+            pynvml, h = self.nvml
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.sample()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -154,11 +217,37 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def sample(self):
+        if not self.nvml:
+            return
+        pynvml, h = self.nvml
+        try:
+            self.sm.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+            bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            return
+        for name, bit in self.NVML_REASONS:
+            if bits & bit:
+                self.reasons.add(name)
+
+    def wait(self, event, every_s=0.002):
+        """Samples every `every_s` seconds until the CUDA event has completed."""
+        self.sample()
+        while not event.query():
+            self.sample()
+            time.sleep(every_s)
+        self.sample()
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        if self.nvml:
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -168,6 +257,11 @@ class ClockSampler:
             self.thread.join(timeout=2)
 
     def summary(self):
+        if self.nvml:
+            if not self.sm:
+                return None
+            return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "NVML, polled every 2 ms"}
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.lines:
@@ -184,7 +278,8 @@ class ClockSampler:
                     reasons.add(n)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvidia-smi -lms 200"}
 
 
 # ---------------------------------------------------------------- GPU side
@@ -241,6 +336,7 @@ def time_engine(e, steps, warmup, world, local):
         for _ in range(steps // k):
             e.step(k)
         stop.record(stream)
+        clk.wait(stop)
         stop.synchronize()
     torch.cuda.synchronize(local)
     ms = start.elapsed_time(stop)
@@ -256,7 +352,7 @@ def run_ours(args):
     w = workload(args.config)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(args.cpu_steps, 2)          # before the first GPU call
+        cpu = cpu_baseline(w, args.cpu_steps, 2, args.cpu_omp_steps)   # before the first GPU call
     t = tissue.box(w["nx"], w["ny"], w["nz"], period=w["period"], seed=1234 + rank)
     n = t.n
     peak, peak_src = read_peaks()
@@ -321,12 +417,10 @@ def run_ours(args):
         "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64 (mixed: FP32 fits/gates/currents/stencil, FP64 Vm and concentrations)",
         "data": "synthetic, seeded (no dataset: the configs define geometry, fibres and pacing)",
-        "config": {"workload": w["label"], "cells_per_gpu": n, "dt_ms": DT, "precision": "mixed",
-                   "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (state + weights %.1f GB per GPU)" % (
-                       (ALGO_BYTES["mixed"] - 16) * n / 1e9),
-                   "timing": "one CUDA graph of %d steps, captured during warm-up, replayed %d times" % (
-                       batch_of(args.steps), args.steps // batch_of(args.steps))},
+        "config": bench_config(w, world),
+        "precision": "mixed",
+        "timing": "one CUDA graph of %d steps, captured during warm-up, replayed %d times" % (
+            batch_of(args.steps), args.steps // batch_of(args.steps)),
         "impl": "ours",
         "roofline": m["roofline"],
         "fp64": {"value": f["value"], "ms_per_step": f["ms_per_step"], "roofline": f["roofline"],
@@ -512,16 +606,21 @@ def time_plain_fp64(t, args, local):
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU path (oracle/_ref) on the
+    same box, timed on the host cores (bench.cpu_baseline); rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     w = workload(args.config)
-    cb = cpu_baseline(args.steps, args.warmup)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    cb = cpu_baseline(w, args.steps, args.warmup, args.cpu_omp_steps)
     line = {
-        "metric": METRIC, "value": cb["value"], "unit": METRIC, "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "metric": METRIC, "value": cb["value"], "unit": METRIC, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic, seeded",
-        "config": {"workload": w["label"], "precision": "fp64 (reference CPU path)"},
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic, seeded (no dataset: the configs define geometry, "
+                                                     "fibres and pacing)",
+        "config": bench_config(w, world),
+        "precision": "fp64 (the reference CPU path)",
         "impl": "reference",
         "cpu_baseline": cb,
         "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -535,7 +634,7 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=["box256", "box128", "box64", "shell", "batch4096", "serve"],
+    ap.add_argument("--config", choices=["box256", "box192", "box128", "box64", "shell", "batch4096", "serve"],
                     default="box256")
     ap.add_argument("--shell-dx", type=float, default=0.25)
     ap.add_argument("--instances", type=int, default=4096)
@@ -545,7 +644,9 @@ def main():
     ap.add_argument("--job-steps", type=int, default=2500)
     ap.add_argument("--serve-batch", type=int, default=250)
     ap.add_argument("--e2e-steps", type=int, default=50)
-    ap.add_argument("--cpu-steps", type=int, default=40)
+    ap.add_argument("--cpu-steps", type=int, default=20, help="steps per CPU slab process (cpu_baseline)")
+    ap.add_argument("--cpu-omp-steps", type=int, default=2,
+                    help="steps of the one-process omp loop on the whole box (0: skip)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--precision", choices=["both", "fp64", "mixed"], default="both",
                     help="profiling runs: time one precision only (no headline line)")

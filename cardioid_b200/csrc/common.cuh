@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/cardioid_b200.h"
 #include "tt06_device.cuh"
@@ -116,13 +117,93 @@ inline bool pack_fits(const cdb_fit* fits, FitShape& sh, double* pool, int poolS
   return true;
 }
 
+// Taylor shift and scale of a polynomial: q with sum_k c_k x^k =
+// sum_j q_j t^j, t = (x - s) / h.  Repeated synthetic division by (x - s)
+// in long double (each coefficient to about 1e-12 relative even where the
+// monomial coefficients cancel strongly), then q_j = a_j h^j.
+inline void taylor_shift(const double* c, int n, double s, double h, long double* q)
+{
+  for (int k = 0; k < n; ++k) q[k] = c[k];
+  for (int i = 0; i < n; ++i)
+    for (int k = n - 2; k >= i; --k) q[k] += (long double)s * q[k + 1];
+  long double hp = 1;
+  for (int j = 0; j < n; ++j, hp *= h) q[j] *= hp;
+}
+
+// FP32 coefficient pool of the mixed kernels from a pool packed at the
+// compiled offsets (pack_fits_spec): a fit in kSpecShiftMask is rewritten in
+// t = (x - kSpecShift) / kSpecShiftScale, numerator and denominator divided
+// by the denominator's constant term so that the denominator keeps the form
+// 1 + t (...); every other fit is the FP32 rounding of its coefficients.
+// False when a shifted denominator vanishes at the shift point.
+inline bool spec_pool32(const double* pool, float* out, int poolSize)
+{
+  for (int k = 0; k < poolSize; ++k) out[k] = (float)pool[k];
+  long double qn[CDB_MAX_COEFF + 1], qd[CDB_MAX_COEFF + 1];
+  double den[CDB_MAX_COEFF + 1];
+  for (int f = 0; f < kNumFits; ++f) {
+    if (!((kSpecShiftMask >> f) & 1u)) continue;
+    const int O = kSpecOffset[f], N = kSpecNumer[f], D = kSpecDenom[f];
+    den[0] = 1.0;
+    for (int k = 1; k < D; ++k) den[k] = pool[O + N + k - 1];
+    taylor_shift(pool + O, N, kSpecShift[f], kSpecShiftScale, qn);
+    taylor_shift(den, D, kSpecShift[f], kSpecShiftScale, qd);
+    if (!(std::fabs((double)qd[0]) > 0.0) || !std::isfinite((double)qd[0])) return false;
+    for (int k = 0; k < N; ++k) out[O + k] = (float)(qn[k] / qd[0]);
+    for (int k = 1; k < D; ++k) out[O + N + k - 1] = (float)(qd[k] / qd[0]);
+  }
+  return true;
+}
+
+// Whether the FP32 forms of spec_pool32, evaluated as the mixed kernels do
+// (FMA Horner in x or in the shifted t, FP32 quotient), stay within 1e-5 of
+// each fit's largest magnitude against the FP64 monomial form over the fit's
+// domain (V in [-100, 100] mV; Ca_ss in [1e-7, 0.1] mM for slot 0).
+inline bool spec_fp32_ok(const double* pool, const float* pool32)
+{
+  for (int f = 0; f < kNumFits; ++f) {
+    const int O = kSpecOffset[f], N = kSpecNumer[f], D = kSpecDenom[f];
+    const bool shifted = (kSpecShiftMask >> f) & 1u;
+    const double lo = f == 0 ? 1e-7 : -100.0, hi = f == 0 ? 0.1 : 100.0;
+    double maxErr = 0, maxVal = 0;
+    const int nPts = 4001;
+    for (int i = 0; i < nPts; ++i) {
+      const double x = lo + (hi - lo) * i / (nPts - 1);
+      double num = pool[O + N - 1];
+      for (int k = N - 2; k >= 0; --k) num = pool[O + k] + x * num;
+      double den = 1;
+      if (D > 1) {
+        den = pool[O + N + D - 2];
+        for (int k = D - 3; k >= 0; --k) den = pool[O + N + k] + x * den;
+        den = 1 + x * den;
+      }
+      const double v = num / den;
+      const float xf = shifted ? std::fma((float)x, 1.0f / kSpecShiftScale, -kSpecShift[f] / kSpecShiftScale)
+                               : (float)x;
+      float nf = pool32[O + N - 1];
+      for (int k = N - 2; k >= 0; --k) nf = std::fma(xf, nf, pool32[O + k]);
+      float df = 1.0f;
+      if (D > 1) {
+        df = pool32[O + N + D - 2];
+        for (int k = D - 3; k >= 0; --k) df = std::fma(xf, df, pool32[O + N + k]);
+        df = std::fma(xf, df, 1.0f);
+      }
+      const float vf = nf / df;
+      maxVal = std::max(maxVal, std::fabs(v));
+      const double e = std::fabs((double)vf - v);
+      maxErr = std::isfinite(e) ? std::max(maxErr, e) : 1e300;
+    }
+    if (maxErr > 1e-5 * maxVal) return false;
+  }
+  return true;
+}
+
 // Packs 30 fits at the compile-time offsets of fit_shapes.h, zero-padded,
-// when every fit is no longer than the compiled shape (and needs FP64 in the
-// mixed path only where the compiled kernel uses it); false otherwise.
+// when every fit is no longer than the compiled shape and the mixed
+// kernels' FP32 forms of them are accurate (spec_fp32_ok); false otherwise.
 inline bool pack_fits_spec(const cdb_fit* fits, double* pool, int poolSize)
 {
   static_assert(kSpecPool <= kFitPoolPerType, "compiled fit pool exceeds the per-type pool");
-  if ((fp64_fit_mask(fits) & ~kSpecFp64Mask) != 0) return false;
   for (int f = 0; f < kNumFits; ++f) {
     const int nn = fits[f].numer, nd = fits[f].denom;
     if (nn < 1 || nd < 1 || nn > kSpecNumer[f]) return false;
@@ -135,7 +216,8 @@ inline bool pack_fits_spec(const cdb_fit* fits, double* pool, int poolSize)
     for (int k = 0; k < nn; ++k) pool[O + k] = fits[f].coeff[k];
     for (int k = 0; k < nd - 1; ++k) pool[O + N + k] = fits[f].coeff[nn + k];
   }
-  return true;
+  std::vector<float> pool32(poolSize);
+  return spec_pool32(pool, pool32.data(), poolSize) && spec_fp32_ok(pool, pool32.data());
 }
 
 inline TT06Scalars to_scalars(const cdb_tt06_params& p)

@@ -143,7 +143,9 @@ int acquire_slot(int device, const TT06Scalars& scal, const FitShape& shape, con
     }
   for (int s = 0; s < CDB_MAX_REACTION_TYPES; ++s) {
     if (used[s].refs > 0) continue;
-    const std::vector<float> pool32(pool.begin(), pool.end());
+    // the compiled kernels' FP32 forms (shifted fits) for a specialised pool
+    std::vector<float> pool32(pool.begin(), pool.end());
+    if (spec && !spec_pool32(pool.data(), pool32.data(), (int)pool.size())) return -1;
     err = cudaMemcpyToSymbol(c_scal, &scal, sizeof(scal), s * sizeof(TT06Scalars));
     if (err == cudaSuccess) err = cudaMemcpyToSymbol(c_shape, &shape, sizeof(shape), s * sizeof(FitShape));
     if (err == cudaSuccess)
@@ -750,6 +752,23 @@ double cdb_fit_eval(const cdb_fit* f, double x)
   for (int k = f->denom - 3; k >= 0; --k) den = d[k] + x * den;
   den = 1 + x * den;
   return num / den;
+}
+
+cdb_status cdb_diag_fit_forms(const cdb_fit fits[CDB_NUM_FITS], int32_t poolSize, float* pool32, float* shift,
+                              float* scale, int32_t* compiled)
+{
+  CDB_CHECK(fits && pool32 && shift && scale && compiled, CDB_INVALID_ARG, "null argument");
+  CDB_CHECK(poolSize >= kSpecPool, CDB_INVALID_ARG, "pool32 holds fewer than the compiled pool's coefficients");
+  std::vector<double> pool(kFitPoolPerType, 0.0);
+  *compiled = pack_fits_spec(fits, pool.data(), kFitPoolPerType) ? 1 : 0;
+  if (*compiled) {
+    std::vector<float> p32(kFitPoolPerType);
+    CDB_CHECK(spec_pool32(pool.data(), p32.data(), kFitPoolPerType), CDB_INVALID_ARG, "shifted denominator vanishes");
+    for (int k = 0; k < kSpecPool; ++k) pool32[k] = p32[k];
+  }
+  for (int f = 0; f < kNumFits; ++f) shift[f] = kSpecShift[f];
+  *scale = kSpecShiftScale;
+  return CDB_OK;
 }
 
 cdb_status cdb_engine_create(const cdb_engine_config* cfg, cdb_engine** out)

@@ -13,8 +13,9 @@
 //          last bits);
 //   mixed  fits, gates, currents and R_prime in FP32; Vm and the five
 //          concentrations in FP64 (their per-step increments are ~1e-7 of
-//          their values); the few fits whose monomial form loses accuracy in
-//          FP32 are evaluated in FP64.
+//          their values).  The compiled kernels evaluate the few fits whose
+//          monomial form loses accuracy in FP32 in a shifted argument
+//          (fit_shift32); the generic kernel evaluates them in FP64.
 // Fit evaluation is a policy: GenericFits reads term counts at run time;
 // SpecFits has them as compile-time constants (fit_shapes.h), so every
 // Horner chain unrolls and the 30 independent chains interleave.
@@ -182,8 +183,9 @@ __device__ __forceinline__ float fit_spec32(const float* __restrict__ c, float x
 // cell (shared by every V-fit), each term is fma(pw[k], c_k, acc), so the
 // coefficient is the multiplicand and can be an immediate constant-bank
 // operand; Horner's form puts it in the addend slot, where it needs a load.
-// Used only for the fits the FP32 error check accepted (well conditioned
-// in the monomial basis, so the two summation orders agree to FP32 rounding).
+// Used only for the fits the FP32 error check accepted as written (well
+// conditioned in the monomial basis, so the two summation orders agree to
+// FP32 rounding).
 constexpr int kMaxPow = 24;
 
 template <int SLOT>
@@ -201,12 +203,27 @@ __device__ __forceinline__ float fit_pow32(const float* __restrict__ c, const fl
   return fdiv(num, den);
 }
 
-// The largest power any FP32-evaluated V-fit of the compiled shapes needs.
+// FP32 fit in the shifted argument t = (x - s) / h of fit_shapes.h (the
+// fits whose monomial form loses accuracy in FP32: their numerator and
+// denominator span many decades over the domain, and about the shift point
+// the Taylor coefficients no longer cancel).  h is a power of two, so t is
+// one FMA with immediate operands and no extra rounding; the coefficients
+// were rewritten in t at registration (spec_pool32).
+template <int SLOT>
+__device__ __forceinline__ float fit_shift32(const float* __restrict__ c, float x)
+{
+  constexpr float inv = 1.0f / kSpecShiftScale, off = -kSpecShift[SLOT] / kSpecShiftScale;
+  return fit_spec32<SLOT>(c, fmaf(x, inv, off));
+}
+
+__host__ __device__ constexpr bool spec_shifted(int slot) { return (kSpecShiftMask >> slot) & 1u; }
+
+// The largest power any power-basis V-fit of the compiled shapes needs.
 __host__ __device__ constexpr int spec_max_pow32()
 {
   int m = 1;
   for (int s = 1; s < 30; ++s) {
-    if (s == 29 || ((kSpecFp64Mask >> s) & 1u)) continue;   // K1 takes V - E_K; FP64 fits use Horner
+    if (s == 29 || spec_shifted(s)) continue;   // K1 takes V - E_K; shifted fits use Horner in t
     const int need = kSpecNumer[s] > kSpecDenom[s] ? kSpecNumer[s] : kSpecDenom[s];
     if (need > m) m = need;
   }
@@ -238,26 +255,29 @@ struct GenericFits {
 struct SpecFits {
   const double* __restrict__ c64;
   const float* __restrict__ c32;
-  float pw[kMaxPow];   // V^k for the FP32 V-fits (set_v)
-  __device__ __forceinline__ void set_v(float v)
+  float pw[kMaxPow];   // V^k for the power-basis V-fits (set_v)
+  float v;             // V in FP32 (set_v)
+  __device__ __forceinline__ void set_v(float vf)
   {
+    v = vf;
     pw[0] = 1.0f;
 #pragma unroll
-    for (int k = 1; k < spec_max_pow32(); ++k) pw[k] = pw[k - 1] * v;
+    for (int k = 1; k < spec_max_pow32(); ++k) pw[k] = pw[k - 1] * vf;
   }
   template <int SLOT>
   __device__ __forceinline__ double f64(double x) const { return fit_spec64<SLOT>(c64, x); }
+  // a fit of another argument (Ca_ss, V - E_K): Horner in x or in t
   template <int SLOT>
-  __device__ __forceinline__ float fmix(float xf, double xd) const
+  __device__ __forceinline__ float fmix(float xf, double) const
   {
-    if ((kSpecFp64Mask >> SLOT) & 1u) return (float)fit_spec64<SLOT>(c64, xd);
+    if (spec_shifted(SLOT)) return fit_shift32<SLOT>(c32, xf);
     return fit_spec32<SLOT>(c32, xf);
   }
-  // a fit of V: the power basis in FP32
+  // a fit of V: the power basis, or Horner in t for the shifted fits
   template <int SLOT>
-  __device__ __forceinline__ float fv(double vd) const
+  __device__ __forceinline__ float fv(double) const
   {
-    if ((kSpecFp64Mask >> SLOT) & 1u) return (float)fit_spec64<SLOT>(c64, vd);
+    if (spec_shifted(SLOT)) return fit_shift32<SLOT>(c32, v);
     return fit_pow32<SLOT>(c32, pw);
   }
 };

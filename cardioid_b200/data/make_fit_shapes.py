@@ -5,13 +5,24 @@ Per fit slot the header holds the largest numerator and denominator term
 counts over the shipped celltypes; a reaction type whose fits are no longer
 than these is packed zero-padded at the header's fixed offsets (leading zero
 coefficients leave Horner's result unchanged) and runs the fully unrolled
-kernel; any other fit set runs the generic kernel.  The header also lists
-the fits the mixed kernel evaluates in FP64 (those whose monomial form
-loses more than 1e-5 of their range in FP32, as decided at registration).
+kernel; any other fit set runs the generic kernel.
+
+The header also holds, per fit, the FP32 form the mixed kernels evaluate:
+fits whose monomial form stays within half the 1e-5 tolerance in FP32
+(relative to their range) are evaluated as written (kSpecShift = 0 and
+their bit in kSpecShiftMask clear), so that registration, which accepts
+up to 1e-5, has a margin; the others (high-degree rational fits whose numerator and
+denominator span many decades: the h and m Rush-Larsen rates, the j rate's
+b, the s rate of the non-endo types, the p_K term and the K1 current) are evaluated in the shifted argument
+t = (x - s) / 128, with s chosen here from a 5 mV grid as the shift giving
+the smallest FP32 error over the shipped celltypes.  Registration rewrites
+those fits' FP32 coefficients in t (common.cuh, spec_pool32).
 
     python -m cardioid_b200.data.make_fit_shapes
 """
 import os
+from fractions import Fraction
+from math import comb
 
 import numpy as np
 
@@ -19,41 +30,78 @@ from cardioid_b200 import engine, tt06
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 HEADER = os.path.join(os.path.dirname(HERE), "csrc", "fit_shapes.h")
+SHIFT_SCALE = 128.0     # a power of two: t = x / 128 - s / 128 is one exactly-scaled FMA
+TOL = 1e-5          # FP32 error allowed, as a fraction of the fit's largest magnitude
 
 
-def fp32_loses(f, slot):
+def domain(slot):
     lo, hi = (1e-7, 0.1) if slot == 0 else (-100.0, 100.0)
-    x = np.linspace(lo, hi, 4001)
-    v = f.eval(x)
-    c = np.array(f.coeff, dtype=np.float32)
-    xf = x.astype(np.float32)
-    num = np.full_like(xf, c[f.numer - 1])
-    for k in range(f.numer - 2, -1, -1):
-        num = (xf * num + c[k]).astype(np.float32)
-    vf = num
-    if f.denom > 1:
-        d = c[f.numer:]
-        den = np.full_like(xf, d[f.denom - 2])
-        for k in range(f.denom - 3, -1, -1):
-            den = (xf * den + d[k]).astype(np.float32)
-        den = (xf * den + 1).astype(np.float32)
-        with np.errstate(all="ignore"):
-            vf = num / den
-    err = np.abs(vf.astype(np.float64) - v)
-    return (not np.isfinite(err).all()) or err.max() > 1e-5 * np.abs(v).max()
+    return np.linspace(lo, hi, 4001)
+
+
+def _horner32(c, x):
+    """FP32 Horner with fused multiply-adds (each step rounded once)."""
+    c = np.asarray(c, np.float32)
+    x = np.asarray(x, np.float32)
+    r = np.full_like(x, c[-1])
+    for a in c[-2::-1]:
+        r = (r.astype(np.float64) * x + np.float64(a)).astype(np.float32)
+    return r.astype(np.float64)
+
+
+def _poly64(c, x):
+    r = np.zeros_like(x)
+    for a in c[::-1]:
+        r = r * x + a
+    return r
+
+
+def taylor_shift(c, s, h=SHIFT_SCALE):
+    """Coefficients q of p(x) = sum_j q_j t^j, t = (x - s) / h, exactly."""
+    q = [Fraction(0)] * len(c)
+    for k, ck in enumerate(c):
+        for j in range(k + 1):
+            q[j] += Fraction(float(ck)) * comb(k, j) * Fraction(float(s)) ** (k - j) * Fraction(h) ** j
+    return np.array([float(v) for v in q])
+
+
+def fp32_error(f, slot, shift=None):
+    """Largest FP32 error of the fit over its domain, relative to its largest
+    magnitude: monomial form (shift None) or shifted form."""
+    x = domain(slot)
+    c = np.array(f.coeff)
+    num, den = c[:f.numer], np.concatenate([[1.0], c[f.numer:]])
+    v = _poly64(num, x) / _poly64(den, x)
+    if shift is None:
+        n32, d32 = _horner32(num, x), _horner32(den, x)
+    else:
+        t = ((x - shift) / SHIFT_SCALE).astype(np.float32)
+        qn, qd = taylor_shift(num, shift), taylor_shift(den, shift)
+        n32, d32 = _horner32(qn / qd[0], t), _horner32(qd / qd[0], t)
+    with np.errstate(all="ignore"):
+        vf = (n32.astype(np.float32) / d32.astype(np.float32)).astype(np.float64)
+        err = np.abs(vf - v).max() / np.abs(v).max()
+    return float(err) if np.isfinite(err) else np.inf
 
 
 def main(dt=0.02):
     numer = [0] * tt06.NFIT
     denom = [0] * tt06.NFIT
+    fits = [engine.default_params(ct, dt).fits for ct in (0, 1, 2)]
+    shift = [0.0] * tt06.NFIT
     mask = 0
-    for ct in (0, 1, 2):
-        p = engine.default_params(ct, dt)
-        for i, f in enumerate(p.fits):
-            numer[i] = max(numer[i], f.numer)
-            denom[i] = max(denom[i], f.denom)
-            if fp32_loses(f, i):
-                mask |= 1 << i
+    for i in range(tt06.NFIT):
+        for fs in fits:
+            numer[i] = max(numer[i], fs[i].numer)
+            denom[i] = max(denom[i], fs[i].denom)
+        if i == 0 or max(fp32_error(fs[i], i) for fs in fits) <= TOL / 2:
+            continue
+        best = min(((max(fp32_error(fs[i], i, s) for fs in fits), s) for s in np.arange(-100.0, 100.1, 5.0)))
+        if best[0] > TOL:
+            raise RuntimeError("fit %d: no shift keeps the FP32 error under %g (best %.3g)" % (i, TOL, best[0]))
+        shift[i] = float(best[1])
+        mask |= 1 << i
+        print("fit %2d: shift %g mV, FP32 error %.3g of range" % (i, shift[i], best[0]))
     offset, off = [], 0
     for i in range(tt06.NFIT):
         offset.append(off)
@@ -67,13 +115,16 @@ def main(dt=0.02):
         "constexpr int kSpecDenom[30] = {%s};" % ", ".join(map(str, denom)),
         "constexpr int kSpecOffset[30] = {%s};" % ", ".join(map(str, offset)),
         "constexpr int kSpecPool = %d;" % off,
-        "constexpr unsigned kSpecFp64Mask = 0x%08xu;" % mask,
+        "// FP32 form of the mixed kernels: fits in kSpecShiftMask take t = (x - kSpecShift) / kSpecShiftScale",
+        "constexpr float kSpecShift[30] = {%s};" % ", ".join("%.1ff" % s for s in shift),
+        "constexpr float kSpecShiftScale = %.1ff;" % SHIFT_SCALE,
+        "constexpr unsigned kSpecShiftMask = 0x%08xu;" % mask,
         "}  // namespace cdb",
         "",
     ]
     with open(HEADER, "w") as f:
         f.write("\n".join(lines))
-    print("wrote", HEADER, "pool", off, "fp64 mask 0x%x" % mask)
+    print("wrote", HEADER, "pool", off, "shift mask 0x%x" % mask)
 
 
 if __name__ == "__main__":

@@ -287,6 +287,16 @@ cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, 
  * measuring it against IEEE division.  No counterpart in the reference. */
 cdb_status cdb_diag_div64(int device, int64_t n, const double* a, const double* b, double* q, void* stream);
 
+/* The fit forms the compiled mixed kernels evaluate (host only, no device
+ * needed): *compiled = 1 when the 30 fits run the compiled (unrolled)
+ * kernels, else 0 (the generic kernel); when compiled, pool32[0..poolSize)
+ * receives their FP32 coefficient pool (the compiled offsets; shifted fits
+ * rewritten in t = (x - shift) / scale), and shift[30] / *scale the
+ * shift of each fit (0 when it is evaluated as written).  No counterpart in
+ * the reference. */
+cdb_status cdb_diag_fit_forms(const cdb_fit fits[CDB_NUM_FITS], int32_t poolSize, float* pool32, float* shift,
+                              float* scale, int32_t* compiled);
+
 /* Launch tuning of the step kernel (no counterpart in the reference):
  * stage 1 = each warp copies its next tile's state (mixed: and weights)
  * into shared memory with cp.async while it computes the current one, 2 =
