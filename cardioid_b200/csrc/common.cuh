@@ -155,15 +155,41 @@ inline bool spec_pool32(const double* pool, float* out, int poolSize)
   return true;
 }
 
+// How the compiled mixed kernels evaluate fit f in FP32: Horner (shifted
+// fits, in t; fits of Ca_ss or V - E_K as written), or the power basis (sum
+// of c_k V^k with V^k by repeated products, low terms first) for the other
+// fits of V.
+inline bool spec_horner32(int f) { return ((kSpecShiftMask >> f) & 1u) || f == 0 || f == 29; }
+
+// One fit's FP32 numerator or denominator polynomial (n coefficients,
+// c[0] the constant term), evaluated in the kernel's order.
+inline float spec_poly32(const float* c, int n, float x, bool horner)
+{
+  if (horner) {
+    float r = c[n - 1];
+    for (int k = n - 2; k >= 0; --k) r = std::fma(x, r, c[k]);
+    return r;
+  }
+  float r = c[0], p = 1.0f;
+  for (int k = 1; k < n; ++k) {
+    p = p * x;
+    r = std::fma(p, c[k], r);
+  }
+  return r;
+}
+
 // Whether the FP32 forms of spec_pool32, evaluated as the mixed kernels do
-// (FMA Horner in x or in the shifted t, FP32 quotient), stay within 1e-5 of
-// each fit's largest magnitude against the FP64 monomial form over the fit's
+// (spec_horner32 / spec_poly32, FP32 quotient), stay within 1e-5 of each
+// fit's largest magnitude against the FP64 monomial form over the fit's
 // domain (V in [-100, 100] mV; Ca_ss in [1e-7, 0.1] mM for slot 0).
 inline bool spec_fp32_ok(const double* pool, const float* pool32)
 {
+  float dc[CDB_MAX_COEFF + 1];
   for (int f = 0; f < kNumFits; ++f) {
     const int O = kSpecOffset[f], N = kSpecNumer[f], D = kSpecDenom[f];
-    const bool shifted = (kSpecShiftMask >> f) & 1u;
+    const bool shifted = (kSpecShiftMask >> f) & 1u, horner = spec_horner32(f);
+    dc[0] = 1.0f;
+    for (int k = 1; k < D; ++k) dc[k] = pool32[O + N + k - 1];
     const double lo = f == 0 ? 1e-7 : -100.0, hi = f == 0 ? 0.1 : 100.0;
     double maxErr = 0, maxVal = 0;
     const int nPts = 4001;
@@ -180,15 +206,7 @@ inline bool spec_fp32_ok(const double* pool, const float* pool32)
       const double v = num / den;
       const float xf = shifted ? std::fma((float)x, 1.0f / kSpecShiftScale, -kSpecShift[f] / kSpecShiftScale)
                                : (float)x;
-      float nf = pool32[O + N - 1];
-      for (int k = N - 2; k >= 0; --k) nf = std::fma(xf, nf, pool32[O + k]);
-      float df = 1.0f;
-      if (D > 1) {
-        df = pool32[O + N + D - 2];
-        for (int k = D - 3; k >= 0; --k) df = std::fma(xf, df, pool32[O + N + k]);
-        df = std::fma(xf, df, 1.0f);
-      }
-      const float vf = nf / df;
+      const float vf = spec_poly32(pool32 + O, N, xf, horner) / spec_poly32(dc, D, xf, horner);
       maxVal = std::max(maxVal, std::fabs(v));
       const double e = std::fabs((double)vf - v);
       maxErr = std::isfinite(e) ? std::max(maxErr, e) : 1e300;

@@ -188,11 +188,11 @@ __device__ __forceinline__ float fit_spec32(const float* __restrict__ c, float x
 // FP32 rounding).
 constexpr int kMaxPow = 24;
 
-template <int SLOT>
-__device__ __forceinline__ float fit_pow32(const float* __restrict__ c, const float (&pw)[kMaxPow])
+template <int SLOT, int P>
+__device__ __forceinline__ float fit_pow32(const float* __restrict__ c, const float (&pw)[P])
 {
   constexpr int N = kSpecNumer[SLOT], D = kSpecDenom[SLOT], O = kSpecOffset[SLOT];
-  static_assert(N <= kMaxPow && D <= kMaxPow, "power table too short");
+  static_assert(N <= P && D <= P, "power table too short");
   float num = c[O];
 #pragma unroll
   for (int k = 1; k < N; ++k) num = fmaf(pw[k], c[O + k], num);
@@ -206,9 +206,11 @@ __device__ __forceinline__ float fit_pow32(const float* __restrict__ c, const fl
 // FP32 fit in the shifted argument t = (x - s) / h of fit_shapes.h (the
 // fits whose monomial form loses accuracy in FP32: their numerator and
 // denominator span many decades over the domain, and about the shift point
-// the Taylor coefficients no longer cancel).  h is a power of two, so t is
-// one FMA with immediate operands and no extra rounding; the coefficients
-// were rewritten in t at registration (spec_pool32).
+// the Taylor coefficients no longer cancel), by Horner in t.  h is a power
+// of two, so t is one FMA with immediate operands and no extra rounding;
+// the coefficients were rewritten in t at registration (spec_pool32).
+// (The power basis of t, with a power table per shift, measured slower:
+// its products cost more than Horner's chains.)
 template <int SLOT>
 __device__ __forceinline__ float fit_shift32(const float* __restrict__ c, float x)
 {

@@ -49,6 +49,27 @@ def _horner32(c, x):
     return r.astype(np.float64)
 
 
+def _pow32(c, x):
+    """FP32 power basis, low terms first: sum of fma(x^k, c_k, acc), x^k by
+    repeated products (each step rounded once)."""
+    c = np.asarray(c, np.float32)
+    x = np.asarray(x, np.float32)
+    p = np.ones_like(x)
+    r = np.full_like(x, c[0])
+    for a in c[1:]:
+        p = (p * x).astype(np.float32)
+        r = (p.astype(np.float64) * np.float64(a) + r).astype(np.float32)
+    return r.astype(np.float64)
+
+
+def horner_slot(slot):
+    """The fits the compiled mixed kernels evaluate by Horner when not
+    shifted (arguments other than V: Ca_ss for slot 0, V - E_K for slot
+    29); the other fits of V in the power basis; every shifted fit by
+    Horner in the shifted argument."""
+    return slot in (0, 29)
+
+
 def _poly64(c, x):
     r = np.zeros_like(x)
     for a in c[::-1]:
@@ -67,13 +88,16 @@ def taylor_shift(c, s, h=SHIFT_SCALE):
 
 def fp32_error(f, slot, shift=None):
     """Largest FP32 error of the fit over its domain, relative to its largest
-    magnitude: monomial form (shift None) or shifted form."""
+    magnitude, evaluated as the compiled mixed kernels do: as written (shift
+    None; Horner or power basis, horner_slot) or by Horner in the shifted
+    argument."""
     x = domain(slot)
     c = np.array(f.coeff)
     num, den = c[:f.numer], np.concatenate([[1.0], c[f.numer:]])
     v = _poly64(num, x) / _poly64(den, x)
     if shift is None:
-        n32, d32 = _horner32(num, x), _horner32(den, x)
+        ev = _horner32 if horner_slot(slot) else _pow32
+        n32, d32 = ev(num, x), ev(den, x)
     else:
         t = ((x - shift) / SHIFT_SCALE).astype(np.float32)
         qn, qd = taylor_shift(num, shift), taylor_shift(den, shift)

@@ -14,11 +14,17 @@ Interpolation::create (elec/Interpolation.cc:115-423):
      best error is under the tolerance;
   4. convert the Chebyshev coefficients to monomials in x and normalise the
      denominator's constant term to 1.
-The least-squares solve is numpy's (LAPACK), where the reference calls
-dgels_; fits are only ever shared through FIT files, so the engine and the
-oracle always evaluate the same coefficients.
+Each least-squares problem is solved as the reference's DGELS call does
+(elec/Interpolation.cc:276-292): Householder QR of the (overdetermined,
+full-rank) matrix, then R x = Q^T y.  The cost search stops at the first
+cost whose best error is under the tolerance, so a solver with different
+rounding (an SVD, say) can stop one cost earlier or later on a fit whose
+error sits at the tolerance; with QR the generated shapes are the
+reference generator's.  Fits are only ever shared through FIT files, so the
+engine and the oracle always evaluate the same coefficients.
 """
 import numpy as np
+from scipy.linalg import solve_triangular
 
 from .tt06 import Fit, NFIT
 
@@ -159,6 +165,12 @@ def _moving_range(y, window):
     return np.maximum(r, r.max() * 1e-7)
 
 
+def _lstsq_qr(A, y):
+    """min ||A x - y||_2 by Householder QR (A of full column rank)."""
+    Q, R = np.linalg.qr(A, mode="reduced")
+    return solve_triangular(R, Q.T @ y)
+
+
 def _cheb_to_mono(c, lb, ub):
     """Chebyshev series on z = (2x - (ub+lb))/(ub-lb) -> monomials in x."""
     n = len(c)
@@ -195,7 +207,7 @@ def fit_samples(x, y, tol, window):
             A[:, :nn] = T[:nn].T
             if nd > 1:
                 A[:, nn:] = (-y[None, :] * T[1:nd]).T
-            coef = np.linalg.lstsq(A, y, rcond=None)[0]
+            coef = _lstsq_qr(A, y)
             num = T[:nn].T @ coef[:nn]
             den = 1 + (T[1:nd].T @ coef[nn:] if nd > 1 else 0)
             err = np.sqrt(np.sum(((y - num / den) / rng) ** 2) / n)

@@ -39,19 +39,14 @@ def offsets():
     return get("kSpecNumer"), get("kSpecDenom"), get("kSpecOffset")
 
 
-def eval32(pool, N, D, O, xf):
-    """FP32 FMA Horner of one packed fit (numerator N terms, denominator
-    1 + x (D - 1 terms)), FP32 quotient."""
-    num = np.full_like(xf, pool[O + N - 1])
-    for k in range(N - 2, -1, -1):
-        num = (num.astype(np.float64) * xf + np.float64(pool[O + k])).astype(np.float32)
-    den = np.ones_like(xf)
-    if D > 1:
-        den = np.full_like(xf, pool[O + N + D - 2])
-        for k in range(D - 3, -1, -1):
-            den = (den.astype(np.float64) * xf + np.float64(pool[O + N + k])).astype(np.float32)
-        den = (den.astype(np.float64) * xf + 1.0).astype(np.float32)
-    return (num / den).astype(np.float64)
+def eval32(pool, N, D, O, xf, horner):
+    """One packed fit (numerator N terms, denominator 1 + x (D - 1 terms))
+    in FP32 as the compiled mixed kernels evaluate it: Horner or the power
+    basis (mfs._horner32 / mfs._pow32), FP32 quotient."""
+    ev = mfs._horner32 if horner else mfs._pow32
+    num = ev(pool[O:O + N], xf)
+    den = ev(np.concatenate([[1.0], pool[O + N:O + N + D - 1]]), xf) if D > 1 else np.ones_like(num)
+    return (num.astype(np.float32) / den.astype(np.float32)).astype(np.float64)
 
 
 @pytest.mark.parametrize("celltype", [0, 1, 2])
@@ -66,7 +61,7 @@ def test_shipped_fits_run_compiled_and_stay_accurate(celltype):
         v = f.eval(x)
         shifted = shift[i] != 0.0
         xf = ((x - shift[i]) / scale).astype(np.float32) if shifted else x.astype(np.float32)
-        vf = eval32(pool, numer[i], denom[i], off[i], xf)
+        vf = eval32(pool, numer[i], denom[i], off[i], xf, horner=mfs.horner_slot(i) or shifted)
         err = np.abs(vf - v).max() / np.abs(v).max()
         assert err <= 1e-5, (i, err)
         if shifted:
