@@ -5,9 +5,12 @@ use it.
   face conductivities   elec/CUDADiffusion.cc:73-122
   flux and its order    elec/CUDADiffusion_ker.cu:16-140 (diff_6face_v1)
 
-Parity unpinned: the reference's own implementation is a CUDA kernel that
-returns from threads before __syncthreads, so it is not run here; this
-restatement follows its code line by line.
+The face conductivities are pinned: tests/test_diff6.py checks face_sigma
+bit for bit against the table the reference's own CUDADiffusion
+constructor builds on the host (run by the oracle build, oracle/_ref).
+The flux is pinned only by restatement: the reference's kernel returns from
+threads before __syncthreads, so it is not run here; calc follows its code
+line by line.
 """
 import numpy as np
 

@@ -26,6 +26,11 @@
 
 #include "Anatomy.hh"
 #include "AnatomyCell.hh"
+// CUDADiffusion keeps its face-conductivity table private; the oracle
+// reads it back to pin the 6-face plugin's table.
+#define private public
+#include "CUDADiffusion.hh"
+#undef private
 #include "FGRDiffusionOMP.hh"
 #include "FGRUtils.hh"
 #include "ReactionManager.hh"
@@ -189,6 +194,28 @@ int ref_sim_use_diffusion_plugin(void* h, const char* path)
    sim->diffusion = f(p, sim->anatomy);
    sim->useDiffusion = true;
    return 0;
+}
+
+// The face-conductivity table that the reference's "cuda" Diffusion builds
+// on the host for the simulation's anatomy (CUDADiffusion constructor,
+// elec/CUDADiffusion.cc:30-130): dims[0..2] = its local grid (the anatomy's
+// bounding box, findBoundingBox(anatomy, false)), dims[3..5] = the grid
+// offset of that box, and out[9 nx ny nz] in its layout, entry
+// z + nz (y + ny (x + nx (j + 3 i))) for face normal i and gradient
+// direction j.  Returns nx ny nz, or -(nx ny nz) (dims still set, out
+// untouched) when out holds fewer than 9 nx ny nz entries.
+long ref_sim_diff6_face_sigma(void* h, int* dims, double* out, long capacity)
+{
+   RefSim* sim = static_cast<RefSim*>(h);
+   CUDADiffusion d(sim->anatomy, 0, sim->diffusionScale);
+   const long n = (long)d.nx_ * d.ny_ * d.nz_;
+   dims[0] = d.nx_; dims[1] = d.ny_; dims[2] = d.nz_;
+   Tuple lo = d.localGrid_.localTuple(Tuple(0, 0, 0));
+   dims[3] = -lo.x(); dims[4] = -lo.y(); dims[5] = -lo.z();
+   if (capacity < 9 * n) return -n;
+   ro_array_ptr<double> f = d.sigmaFaceNormal_.readonly(CPU);
+   for (long k = 0; k < 9 * n; ++k) out[k] = f[k];
+   return n;
 }
 
 void ref_sim_destroy(void* h)

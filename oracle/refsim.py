@@ -50,6 +50,8 @@ def lib():
         L.ref_sim_step.argtypes = [vp, ctypes.c_int]
         L.ref_sim_use_diffusion_plugin.argtypes = [vp, ctypes.c_char_p]
         L.ref_sim_use_diffusion_plugin.restype = ctypes.c_int
+        L.ref_sim_diff6_face_sigma.argtypes = [vp, ip, dp, ctypes.c_long]
+        L.ref_sim_diff6_face_sigma.restype = ctypes.c_long
         L.ref_set_threads.argtypes = [ctypes.c_int]
         L.ref_read_pio.restype = ctypes.c_long
         L.ref_read_pio.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_int, dp,
@@ -147,6 +149,21 @@ class RefSim:
         out = np.empty(self.n)
         lib().ref_sim_get_activation(self.h, _dp(out))
         return out
+
+    def diff6_face_sigma(self, gid_xyz):
+        """The face-conductivity table the reference's CUDADiffusion builds
+        for this anatomy (elec/CUDADiffusion.cc:73-122), read back at the
+        given cells: [n, 3, 3], [cell, face normal i, gradient direction j].
+        gid_xyz = (x, y, z) global tuples of the cells."""
+        dims = (ctypes.c_int * 6)()
+        lib().ref_sim_diff6_face_sigma(self.h, dims, None, 0)        # sizes only
+        nx, ny, nz = dims[0], dims[1], dims[2]
+        table = np.empty(9 * nx * ny * nz)
+        if lib().ref_sim_diff6_face_sigma(self.h, dims, _dp(table), table.size) < 0:
+            raise RuntimeError("face table larger than expected")
+        t = table.reshape(3, 3, nx, ny, nz)        # [i][j][x][y][z]
+        x, y, z = (np.asarray(c) - dims[3 + k] for k, c in enumerate(gid_xyz))
+        return np.ascontiguousarray(np.moveaxis(t[:, :, x, y, z], -1, 0))
 
     def field_names(self):
         buf = ctypes.create_string_buffer(4096)

@@ -1,7 +1,14 @@
 """The "cuda" 6-face diffusion plugin (cdb_diff6_*) against the oracle's
 numpy restatement of CUDADiffusion (oracle/diff6.py): face conductivities
 and dVm on a box with rotated fibres and on an irregular mask, within 1e-12
-of the largest |dVm| (the GPU may contract products into FMAs)."""
+of the largest |dVm| (the GPU may contract products into FMAs).
+
+The face-conductivity table is pinned to the reference's own code: the
+oracle build constructs the reference's CUDADiffusion (its constructor
+builds the table on the host, elec/CUDADiffusion.cc:73-122), and both the
+restatement (CPU) and the plugin (GPU) reproduce it bit for bit.  The
+reference's kernel (diff_6face_v1) is not run: it returns from threads
+before a __syncthreads."""
 import numpy as np
 import pytest
 
@@ -16,6 +23,31 @@ def _tissues():
     masked = tissue.Tissue(box.nx, box.ny, box.nz, box.dx, box.dy, box.dz, box.gid[keep], box.cell_type[keep],
                            box.sigma[keep], box.vm0[keep], [])
     return {"box": box, "masked": masked}
+
+
+def _ref_built():
+    from oracle import refsim
+    return refsim.available()
+
+
+def _reference_faces(t):
+    """The reference CUDADiffusion's face table at t's cells (diffusion
+    scale t.diffusion_scale)."""
+    from golden.make_golden import reference_sim
+    sim = reference_sim(t)
+    try:
+        return sim.diff6_face_sigma(t.tuples())
+    finally:
+        sim.close()
+
+
+@pytest.mark.skipif(not _ref_built(), reason="needs the reference build (oracle/_ref)")
+@pytest.mark.parametrize("kind", ["box", "masked"])
+def test_oracle_face_table_is_the_references(kind):
+    from oracle import diff6
+    t = _tissues()[kind]
+    ref = _reference_faces(t)
+    np.testing.assert_array_equal(diff6.face_sigma(t, t.diffusion_scale), ref)
 
 
 def test_oracle_face_rule_on_a_uniform_box():
@@ -44,6 +76,9 @@ def test_diff6_plugin_matches_oracle(cdb_lib, kind):
     vm = -80.0 + 40.0 * rng.random(t.n)
     d = plugins.CUDADiffusion(t, 714.2857)
     np.testing.assert_allclose(d.face_sigma(), diff6.face_sigma(t, 714.2857), rtol=1e-15, atol=0)
+    if _ref_built():
+        d2 = plugins.CUDADiffusion(t, t.diffusion_scale)
+        np.testing.assert_array_equal(d2.face_sigma(), _reference_faces(t))
     V = torch.tensor(vm, device="cuda")
     out = torch.empty_like(V)
     d.updateLocalVoltage(V)
