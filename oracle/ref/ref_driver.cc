@@ -46,6 +46,9 @@
 #include "pio.h"
 
 Stimulus* stimulusFactory(const std::string& name, const Anatomy& anatomy);
+// The reference's CPU ECG sum (elec/ECGSensor.cc:231-246; not in a header).
+void calcEcg(rw_mgarray_ptr<double> ecgs, ro_mgarray_ptr<double> invr, ro_mgarray_ptr<double> dVmDiffusion,
+             const int nEcgPoints);
 
 namespace {
 
@@ -216,6 +219,26 @@ long ref_sim_diff6_face_sigma(void* h, int* dims, double* out, long capacity)
    ro_array_ptr<double> f = d.sigmaFaceNormal_.readonly(CPU);
    for (long k = 0; k < 9 * n; ++k) out[k] = f[k];
    return n;
+}
+
+// ecgs[j] = sum over cells i of invr[i nPoints + j] dVmD[i], by the
+// reference's CPU ECG sum calcEcg (elec/ECGSensor.cc:231-246) on arrays in
+// its layout; ecgs starts at zero (ECGSensor::eval zeroes it first).
+void ref_calc_ecg(long nCells, int nPoints, const double* invr, const double* dVmD, double* ecgs)
+{
+   lazy_array<double> e, r, d;
+   e.resize(nPoints);
+   r.resize(nCells * nPoints);
+   d.resize(nCells);
+   {
+      wo_array_ptr<double> ee = e.writeonly(CPU), rr = r.writeonly(CPU), dd = d.writeonly(CPU);
+      for (int j = 0; j < nPoints; ++j) ee[j] = 0;
+      for (long k = 0; k < nCells * nPoints; ++k) rr[k] = invr[k];
+      for (long k = 0; k < nCells; ++k) dd[k] = dVmD[k];
+   }
+   calcEcg(e, r, d, nPoints);
+   ro_array_ptr<double> out = e.readonly(CPU);
+   for (int j = 0; j < nPoints; ++j) ecgs[j] = out[j];
 }
 
 void ref_sim_destroy(void* h)

@@ -52,6 +52,7 @@ def lib():
         L.ref_sim_use_diffusion_plugin.restype = ctypes.c_int
         L.ref_sim_diff6_face_sigma.argtypes = [vp, ip, dp, ctypes.c_long]
         L.ref_sim_diff6_face_sigma.restype = ctypes.c_long
+        L.ref_calc_ecg.argtypes = [ctypes.c_long, ctypes.c_int, dp, dp, dp]
         L.ref_set_threads.argtypes = [ctypes.c_int]
         L.ref_read_pio.restype = ctypes.c_long
         L.ref_read_pio.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_int, dp,
@@ -182,6 +183,17 @@ class RefSim:
         v = np.ascontiguousarray(values, dtype=np.float64)
         if lib().ref_sim_set_state(self.h, name.encode(), _dp(v)) != 0:
             raise KeyError(name)
+
+
+def calc_ecg(invr, dvmd):
+    """The reference's CPU ECG sum (calcEcg, elec/ECGSensor.cc:231-246):
+    ecgs[j] = sum over cells i (in order) of invr[i, j] dvmd[i]."""
+    invr = np.ascontiguousarray(invr, dtype=np.float64)
+    dvmd = np.ascontiguousarray(dvmd, dtype=np.float64)
+    n, m = invr.shape
+    out = np.empty(m)
+    lib().ref_calc_ecg(n, m, _dp(invr), _dp(dvmd), _dp(out))
+    return out
 
 
 def set_threads(n):

@@ -2,7 +2,10 @@
 (ECGSensor::calcInvR / eval / calcEcg, elec/ECGSensor.cc:46-78 and 231-320):
 ecg_j = kconst dx dy dz sum over cells of dVmD / |r - p_j|, r = (x dx, y dy,
 z dz), evaluated every evalRate steps on that step's dVmD.  The oracle's
-dVmD (oracle port) feeds a numpy restatement of that sum.
+dVmD (oracle port) feeds a numpy restatement of that rule: the 1/r table of
+the reference's calcInvr kernel (elec/ECGSensor.cu:9-40, restated: it is
+CUDA code) and the sum, which is pinned on the CPU to the reference's own
+calcEcg run by the oracle build.
 
 Tolerance: FP64 relative 1e-9 of the largest |ecg| (the sum runs in another
 order); mixed relative 2e-3."""
@@ -11,19 +14,51 @@ import pytest
 
 from cardioid_b200 import tissue
 
-pytestmark = pytest.mark.gpu
-
 POINTS = np.array([[-2.0, 1.0, 1.2], [1.5, 1.4, 3.0], [5.0, -1.0, 0.7], [1.1, 1.3, 1.0]])
 KCONST = 0.37
 
 
-def ecg_reference(t, dvmd, points, kconst):
+def _ref_built():
+    from oracle import refsim
+    return refsim.available()
+
+
+def invr_table(t, points):
+    """[cell, electrode] 1 / |r - p| with r = (x dx, y dy, z dz) from the
+    cell's gid (the reference's calcInvr_kernel)."""
     x, y, z = t.tuples()
     r = np.stack([x * t.dx, y * t.dy, z * t.dz], axis=1)
-    d = np.linalg.norm(r[:, None, :] - points[None, :, :], axis=2)
-    return kconst * t.dx * t.dy * t.dz * (dvmd[:, None] / d).sum(axis=0)
+    return 1.0 / np.sqrt(((r[:, None, :] - points[None, :, :]) ** 2).sum(axis=2))
 
 
+def ecg_sum(invr, dvmd):
+    """ecg_j = sum_i invr[i, j] dvmd[i] (the reference's calcEcg)."""
+    return (invr * dvmd[:, None]).sum(axis=0)
+
+
+def ecg_reference(t, dvmd, points, kconst):
+    return kconst * t.dx * t.dy * t.dz * ecg_sum(invr_table(t, points), dvmd)
+
+
+@pytest.mark.skipif(not _ref_built(), reason="needs the reference build (oracle/_ref)")
+def test_ecg_sum_is_the_references():
+    """The restatement's sum against the reference's calcEcg on a 1/r table
+    of a masked box and random dVmD: within 1e-13 of the sum of |terms|
+    (numpy sums pairwise, the reference in cell order)."""
+    from oracle import refsim
+    t = tissue.box(13, 9, 7, seed=2)
+    keep = np.random.default_rng(5).random(t.n) > 0.2
+    t = tissue.Tissue(t.nx, t.ny, t.nz, t.dx, t.dy, t.dz, t.gid[keep], t.cell_type[keep], t.sigma[keep],
+                      t.vm0[keep], [])
+    invr = invr_table(t, POINTS)
+    dvmd = np.random.default_rng(6).normal(size=t.n)
+    want = refsim.calc_ecg(invr, dvmd)
+    got = ecg_sum(invr, dvmd)
+    bound = 1e-13 * (np.abs(invr) * np.abs(dvmd)[:, None]).sum(axis=0)
+    assert (np.abs(got - want) <= bound).all(), np.abs(got - want) / bound
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("mixed", 2e-3)])
 def test_fused_ecg_matches_reference_rule(cdb_lib, oracle_port, fits002, precision, tol):
     from cardioid_b200 import engine as eng_mod
@@ -56,6 +91,7 @@ def test_fused_ecg_matches_reference_rule(cdb_lib, oracle_port, fits002, precisi
     assert np.abs(got - want).max() <= tol * scale, np.abs(got - want).max() / scale
 
 
+@pytest.mark.gpu
 def test_ecg_ring_keeps_the_latest_evaluations(cdb_lib, fits002):
     from cardioid_b200 import engine as eng_mod
     t = tissue.box(8, 6, 5)
