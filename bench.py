@@ -412,6 +412,11 @@ def run_ours(args):
               "activation_max_err_ms": float(np.abs(af[both] - am[both]).max()) if both.any() else None,
               "full_beat": apd_check(local) if world == 1 and not args.no_apd else None}
     plain = time_plain_fp64(t, args, local) if world == 1 and not args.no_plain else None
+    # configs 2 and 4 in the same line (one GPU only, to keep the run short)
+    shell_line = shell_block(args.shell_steps, args.shell_dx, world, rank, local) \
+        if world == 1 and not args.no_shell else None
+    serve_line = serve_block(args.line_jobs, args.rate, args.job_steps, args.job_beats, ("mixed",), args.serve_batch,
+                             world, rank, local) if world == 1 and not args.no_serve else None
     line = {
         "metric": METRIC, "value": m["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
@@ -430,6 +435,8 @@ def run_ours(args):
         "plain_fp64": plain,
         "mixed_over_plain_fp64": (m["value"] / plain["value"]) if plain else None,
         "e2e": results["e2e"],
+        "shell": shell_line,
+        "serve": serve_line,
         "gpu_launches": m["gpu_launches"],
         "clocks": m["clocks"],
         "clocks_fp64": f["clocks"],
@@ -443,37 +450,42 @@ def _timed_run(e, steps, warmup, world, local):
     return max_over_ranks(ms, world, local), launches, clocks
 
 
-def run_shell(args):
-    """Irregular anatomy: the truncated prolate-ellipsoid shell at 0.25 mm
-    (20 paced endocardial sites), FP64 and mixed, and the mixed path's
-    activation-time error against FP64 over the timed steps."""
-    world, rank, local = dist_setup()
-    import torch
-    torch.cuda.set_device(local)
+def shell_block(steps, dx, world, rank, local, warmup=3):
+    """Irregular anatomy (config 2): the truncated prolate-ellipsoid shell at
+    dx mm (20 paced endocardial sites), FP64 and mixed, each timed over
+    `steps` steps after `warmup`, and the mixed path's activation-time error
+    against FP64 over those steps."""
     from cardioid_b200 import engine, shell
-    t = shell.prolate_shell(dx=args.shell_dx, seed=1234 + rank)
+    t = shell.prolate_shell(dx=dx, seed=1234 + rank)
     rx = (t.cell_type - 100).astype(np.uint8)
     out, acts = {}, {}
     for prec in ("fp64", "mixed"):
         with engine.Engine(DT, precision=prec, device=local) as e:
             rid = [e.add_reaction(engine.default_params(c, DT)) for c in (0, 1, 2)]
             tid = e.add_tissue(t, np.array(rid, np.uint8)[rx])
-            ms, launches, clocks = _timed_run(e, args.steps, 3, world, local)
+            ms, launches, clocks = _timed_run(e, steps, warmup, world, local)
             acts[prec] = e.read_activation(tid)
-            out[prec] = {"value": world * t.n * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+            out[prec] = {"value": world * t.n * steps / (ms / 1e3), "ms_per_step": ms / steps,
                          "gpu_launches": launches, "clocks": clocks}
     a, b = acts["fp64"], acts["mixed"]
     both = (a > 0) & (b > 0)
-    if rank == 0:
-        print(json.dumps({
-            "metric": METRIC, "unit": METRIC, "workload": "prolate shell %.3g mm: %d cells on a %dx%dx%d grid, "
-            "20 paced endocardial sites, steps %d (+3 warm-up) at dt %g" % (args.shell_dx, t.n, t.nx, t.ny, t.nz,
-                                                                          args.steps, DT),
+    return {"metric": METRIC, "unit": METRIC,
+            "workload": "prolate shell %.3g mm (config 2): %d cells on a %dx%dx%d grid, 64-bit voxel indices, "
+                        "20 paced endocardial sites, %d steps (+%d warm-up) at dt %g"
+                        % (dx, t.n, t.nx, t.ny, t.nz, steps, warmup, DT),
             "n_gpus": world, "fp64": out["fp64"], "mixed": out["mixed"],
             "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
             "mixed_vs_fp64": {"activated_fp64": int((a > 0).sum()), "activated_mixed": int((b > 0).sum()),
-                              "activation_max_err_ms": float(np.abs(a[both] - b[both]).max()) if both.any() else None}}),
-            flush=True)
+                              "activation_max_err_ms": float(np.abs(a[both] - b[both]).max()) if both.any() else None}}
+
+
+def run_shell(args):
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    line = shell_block(args.steps, args.shell_dx, world, rank, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def run_batch(args):
@@ -505,27 +517,38 @@ def run_batch(args):
                           % (len(insts), pop.total_cells(insts), args.steps, DT), **out}), flush=True)
 
 
-def run_serve(args):
-    """Serving: Poisson job arrivals, continuous batching in one engine;
-    p50/p99 time-to-result and aggregate cell-steps/s."""
-    world, rank, local = dist_setup()
-    import torch
-    torch.cuda.set_device(local)
+def serve_block(n_jobs, rate, job_steps, job_beats, precisions, serve_batch, world, rank, local):
+    """Serving (config 4): Poisson job arrivals with config 4's size and
+    parameter distributions, continuous batching in one engine per
+    precision; p50/p99 time-to-result and aggregate cell-steps/s.  Each job
+    runs `job_beats` paced beats, or `job_steps` steps when that is given
+    (a shortened job, labelled so)."""
     from cardioid_b200 import engine, serving
-    spec = serving.JobSpec(rate=args.rate, steps=args.job_steps)
-    jobs = serving.partition(serving.draw_jobs(args.jobs, spec, seed=1234), rank, world)
+    spec = serving.JobSpec(rate=rate, steps=job_steps or None, beats=job_beats)
+    jobs = serving.partition(serving.draw_jobs(n_jobs, spec, seed=1234), rank, world)
     out = {}
-    for prec in ("mixed", "fp64"):
+    for prec in precisions:
         with engine.Engine(DT, precision=prec, device=local) as e:
             rid = [e.add_reaction(engine.default_params(c, DT)) for c in (0, 1, 2)]
-            srv = serving.Server(e, rid, batch=args.serve_batch)
+            srv = serving.Server(e, rid, batch=serve_batch)
             res = srv.run(jobs)
             out[prec] = serving.summary(res, srv.elapsed, srv.cell_steps)
             out[prec]["rejected"] = len(srv.rejected)
+    length = ("%d steps (%g ms of simulated time, shortened from config 4's %d paced beats)"
+              % (job_steps, job_steps * DT, job_beats) if job_steps else "%d paced beats" % job_beats)
+    return {"metric": "time-to-result p50/p99 (s), cell-steps/s", "n_gpus": world,
+            "workload": "serving (config 4): %d jobs, Poisson %.3g/s, log-normal sizes (median 2e5, max 3e7 cells), "
+                        "each %s at dt %g" % (n_jobs, rate, length, DT), **out}
+
+
+def run_serve(args):
+    world, rank, local = dist_setup()
+    import torch
+    torch.cuda.set_device(local)
+    line = serve_block(args.jobs, args.rate, args.job_steps, args.job_beats, ("mixed", "fp64"), args.serve_batch,
+                       world, rank, local)
     if rank == 0:
-        print(json.dumps({"metric": "time-to-result p50/p99 (s), cell-steps/s", "n_gpus": world,
-                          "workload": "%d jobs, Poisson %.3g/s, log-normal sizes (median 2e5, max 3e7 cells), "
-                          "%d steps each at dt %g" % (args.jobs, args.rate, args.job_steps, DT), **out}), flush=True)
+        print(json.dumps(line), flush=True)
 
 
 def apd_check(local, n=32, steps=20000, every=10, probes=64):
@@ -639,9 +662,15 @@ def main():
     ap.add_argument("--shell-dx", type=float, default=0.25)
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--batch-precisions", default="mixed,fp64")
-    ap.add_argument("--jobs", type=int, default=200)
-    ap.add_argument("--rate", type=float, default=5.0)
-    ap.add_argument("--job-steps", type=int, default=2500)
+    ap.add_argument("--jobs", type=int, default=200, help="jobs of --config serve")
+    ap.add_argument("--line-jobs", type=int, default=24, help="jobs of the serving block in the headline line")
+    ap.add_argument("--rate", type=float, default=5.0, help="job arrivals per second (serving)")
+    ap.add_argument("--job-steps", type=int, default=2500,
+                    help="steps per served job (0: the full --job-beats paced beats)")
+    ap.add_argument("--job-beats", type=int, default=5)
+    ap.add_argument("--shell-steps", type=int, default=100, help="timed steps of the shell block in the headline line")
+    ap.add_argument("--no-shell", action="store_true", help="skip the shell (config 2) block of the headline line")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving (config 4) block of the headline line")
     ap.add_argument("--serve-batch", type=int, default=250)
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--cpu-steps", type=int, default=20, help="steps per CPU slab process (cpu_baseline)")
