@@ -284,6 +284,12 @@ def load(paths, simulate=None, generate=None):
                       sigma_t=objectdb.get_float(cond, "sigmaTi", 0.0315e-3))
         elif cmethod == "uniform":
             kw.update(conductivity="uniform")
+        elif cmethod == "JHU":
+            kw.update(conductivity="JHU", sigma_l=objectdb.get_float(cond, "sigmaLi", 0.3e-3),
+                      sigma_t=objectdb.get_float(cond, "sigmaTi", 0.0315e-3),
+                      jhu=dict(sheet_angle=objectdb.get_float(cond, "sheetAngle", 45.0),
+                               rotation_matrix=int(objectdb.get_float(cond, "rotatationMatrix", 1)),
+                               homogeneous_fiber=bool(objectdb.get_float(cond, "homogeneousFiber", 0))))
         t = anatomy_mod.read_anatomy(os.path.join(base, fname), **kw)
         if cmethod == "uniform":
             t.sigma = _uniform_sigma(cond, t.n)

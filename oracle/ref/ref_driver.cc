@@ -26,6 +26,7 @@
 
 #include "Anatomy.hh"
 #include "AnatomyCell.hh"
+#include "JHUConductivity.hh"
 // CUDADiffusion keeps its face-conductivity table private; the oracle
 // reads it back to pin the 6-face plugin's table.
 #define private public
@@ -239,6 +240,31 @@ void ref_calc_ecg(long nCells, int nPoints, const double* invr, const double* dV
    calcEcg(e, r, d, nPoints);
    ro_array_ptr<double> out = e.readonly(CPU);
    for (int j = 0; j < nPoints; ++j) ecgs[j] = out[j];
+}
+
+// Conductivity tensors of the reference's JHU rule (JHUConductivity::compute,
+// elec/JHUConductivity.cc:26-120) for cells `gid` of an nx*ny*nz grid, with
+// the parameters setConductivity gives it (elec/setConductivity.cc:207-226,
+// transmural axis ny - 2); out[6 n] = a11 a12 a13 a22 a23 a33 per cell.
+void ref_jhu_sigma(int nx, int ny, int nz, double sigmaLi, double sigmaTi, double sheetAngle, int rotationMatrix,
+                   int homogeneousFiber, long n, const long long* gid, double* out)
+{
+   JHUConductivityParms p;
+   p.nx = nx; p.ny = ny; p.nz = nz;
+   p.transmuralAxis = ny - 2;
+   p.sigmaLi = sigmaLi;
+   p.sigmaTi = sigmaTi;
+   p.sheetAngle = sheetAngle;
+   p.rotatationMatrix = rotationMatrix;
+   p.homogeneousFiber = homogeneousFiber != 0;
+   JHUConductivity jhu(p);
+   for (long ii = 0; ii < n; ++ii) {
+      AnatomyCell c;
+      c.gid_ = gid[ii];
+      jhu.compute(c);
+      const double v[6] = {c.sigma_.a11, c.sigma_.a12, c.sigma_.a13, c.sigma_.a22, c.sigma_.a23, c.sigma_.a33};
+      for (int k = 0; k < 6; ++k) out[6 * ii + k] = v[k];
+   }
 }
 
 void ref_sim_destroy(void* h)

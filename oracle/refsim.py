@@ -53,6 +53,8 @@ def lib():
         L.ref_sim_diff6_face_sigma.argtypes = [vp, ip, dp, ctypes.c_long]
         L.ref_sim_diff6_face_sigma.restype = ctypes.c_long
         L.ref_calc_ecg.argtypes = [ctypes.c_long, ctypes.c_int, dp, dp, dp]
+        L.ref_jhu_sigma.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_long, lp, dp]
         L.ref_set_threads.argtypes = [ctypes.c_int]
         L.ref_read_pio.restype = ctypes.c_long
         L.ref_read_pio.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), ctypes.c_char_p, ctypes.c_int, dp,
@@ -193,6 +195,16 @@ def calc_ecg(invr, dvmd):
     n, m = invr.shape
     out = np.empty(m)
     lib().ref_calc_ecg(n, m, _dp(invr), _dp(dvmd), _dp(out))
+    return out
+
+
+def jhu_sigma(gid, nx, ny, nz, sigma_l, sigma_t, sheet_angle=45.0, rotation_matrix=1, homogeneous_fiber=False):
+    """Conductivity tensors [n, 6] of the reference's JHUConductivity::compute
+    (elec/JHUConductivity.cc:26-120) for the given cells."""
+    gid = np.ascontiguousarray(gid, dtype=np.int64)
+    out = np.empty((len(gid), 6))
+    lib().ref_jhu_sigma(nx, ny, nz, sigma_l, sigma_t, sheet_angle, rotation_matrix, 1 if homogeneous_fiber else 0,
+                        len(gid), gid.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), _dp(out))
     return out
 
 

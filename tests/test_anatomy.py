@@ -93,3 +93,27 @@ def test_engine_reproduces_reference_multiple_reaction_traces(cdb_lib):
         got = _run(e.step, lambda: e.read_vm(tid), every, len(traces), pos)
     err = np.abs(got - traces[:, 1:]).max()
     assert err <= TRACE_TOL_FP64, err
+
+
+@pytest.mark.skipif(not (lambda: __import__("oracle.refsim", fromlist=["x"]).available())(),
+                    reason="needs the reference build (oracle/_ref)")
+@pytest.mark.parametrize("rot,homog,sheet", [(1, False, 45.0), (1, False, 30.0), (1, True, 45.0)])
+def test_jhu_conductivity_is_the_references(rot, homog, sheet):
+    """anatomy.jhu_sigma against the reference's JHUConductivity::compute
+    (built into the oracle), bit for bit, on every cell of a 7 x 11 x 5
+    grid, for two sheet angles and the homogeneous fibre."""
+    from cardioid_b200 import anatomy
+    from oracle import refsim
+    nx, ny, nz = 7, 11, 5
+    gid = np.arange(nx * ny * nz)
+    want = refsim.jhu_sigma(gid, nx, ny, nz, 0.3e-3, 0.0315e-3, sheet, rot, homog)
+    got = anatomy.jhu_sigma(gid, nx, ny, nz, 0.3e-3, 0.0315e-3, sheet, rot, homog)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_jhu_reflection_convention_is_rejected():
+    """Rotation convention 0 is a reflection; the reference's determinant
+    assert aborts on it, anatomy.jhu_sigma raises."""
+    from cardioid_b200 import anatomy
+    with pytest.raises(ValueError, match="determinant"):
+        anatomy.jhu_sigma(np.arange(10), 7, 11, 5, rotation_matrix=0)
