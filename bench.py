@@ -361,6 +361,9 @@ def run_ours(args):
     finals = {}
     for prec in precs:
         with engine.Engine(DT, precision=prec, device=local) as e:
+            if args.stage is not None or args.ctas is not None:
+                st, ct = e.get_tuning()
+                e.set_tuning(st if args.stage is None else args.stage, ct if args.ctas is None else args.ctas)
             rx, _ = engine.transmural_setup(e, t, DT)
             e.add_tissue(t, rx)
             ms, launches, clocks = time_engine(e, args.steps, args.warmup, world, local)
@@ -371,6 +374,7 @@ def run_ours(args):
             traffic_pc = read_traffic(prec)
             results[prec] = {
                 "value": world * n * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                "tuning": {"stage": e.get_tuning()[0], "ctas_per_sm": e.get_tuning()[1]},
                 "gpu_launches": launches, "clocks": clocks,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_source": peak_src,
@@ -496,12 +500,32 @@ def run_batch(args):
     import torch
     torch.cuda.set_device(local)
     from cardioid_b200 import engine, population as pop
+    from cardioid_b200 import autotune
     insts = pop.draw(pop.PopulationSpec(n=args.instances), seed=1234)
     mine = [i for i in insts if i.index % world == rank]
     out = {}
     for prec in args.batch_precisions.split(","):
+        choice = None
+        if not args.no_autotune:
+            # tile layout, staging and grid chosen on a sample of the population
+            sample = mine[::max(1, len(mine) // 96)]
+
+            def make():
+                e = engine.Engine(DT, precision=prec, device=local)
+                for c in (0, 1, 2):
+                    e.add_reaction(engine.default_params(c, DT))
+                return e
+
+            def add(e):
+                for inst in sample:
+                    t = pop.build(inst)
+                    e.add_tissue(t, np.full(t.n, inst.celltype, np.uint8), scales=inst.scales)
+
+            choice = autotune.tune(make, add, "population-%d" % args.instances)
         with engine.Engine(DT, precision=prec, device=local) as e:
             rid = [e.add_reaction(engine.default_params(c, DT)) for c in (0, 1, 2)]
+            if choice:
+                autotune.apply(e, choice)
             t0 = time.perf_counter()
             for inst in mine:
                 t = pop.build(inst)
@@ -510,7 +534,10 @@ def run_batch(args):
             ms, launches, clocks = _timed_run(e, args.steps, 3, world, local)
             # every rank steps its share; the time is the slowest rank's
             out[prec] = {"value": pop.total_cells(insts) * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
-                         "gpu_launches": launches, "setup_s": setup, "clocks": clocks}
+                         "gpu_launches": launches, "setup_s": setup, "clocks": clocks,
+                         "tuning": {"layout": e.get_layout(), "stage": e.get_tuning()[0],
+                                    "ctas_per_sm": e.get_tuning()[1],
+                                    "autotune_table_ms_per_step": choice["table"] if choice else None}}
     if rank == 0:
         print(json.dumps({"metric": METRIC, "unit": METRIC, "n_gpus": world,
                           "workload": "population of %d instances (%d cells), steps %d (+3 warm-up) at dt %g"
@@ -662,6 +689,7 @@ def main():
     ap.add_argument("--shell-dx", type=float, default=0.25)
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--batch-precisions", default="mixed,fp64")
+    ap.add_argument("--no-autotune", action="store_true", help="config 3: keep the default tile layout and launch")
     ap.add_argument("--jobs", type=int, default=200, help="jobs of --config serve")
     ap.add_argument("--line-jobs", type=int, default=24, help="jobs of the serving block in the headline line")
     ap.add_argument("--rate", type=float, default=5.0, help="job arrivals per second (serving)")
@@ -682,6 +710,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="profiling runs: skip the end-to-end loop")
     ap.add_argument("--no-apd", action="store_true", help="skip the full-beat APD90 comparison (mixed vs FP64)")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 plugin path")
+    ap.add_argument("--stage", type=int, choices=[0, 1, 2, 3], default=None,
+                    help="profiling runs: the step kernel's staging mode (default: the engine's)")
+    ap.add_argument("--ctas", type=int, default=None, help="profiling runs: CTAs per SM of the persistent grid")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

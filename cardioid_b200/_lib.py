@@ -137,6 +137,8 @@ def load():
         "cdb_engine_launch_count": (st, [vp, i64p]),
         "cdb_engine_set_tuning": (st, [vp, ctypes.c_int32, ctypes.c_int32]),
         "cdb_engine_get_tuning": (st, [vp, i32p, i32p]),
+        "cdb_engine_set_layout": (st, [vp, ctypes.c_int32]),
+        "cdb_engine_get_layout": (st, [vp, i32p]),
         "cdb_diag_div64": (st, [ctypes.c_int, ctypes.c_int64, vp, vp, vp, vp]),
         "cdb_engine_stream": (st, [vp, vpp]),
         "cdb_diag_fit_forms": (st, [ctypes.POINTER(Fit), ctypes.c_int32, ctypes.POINTER(ctypes.c_float),

@@ -23,6 +23,7 @@
 // A warp-tile table, grouped by reaction type, maps each warp to one block
 // (step_kernel.cuh).
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
@@ -204,15 +205,18 @@ struct Engine {
   int stage = 1;           // 1: stage each warp's next tile through shared memory (cp.async)
   bool withhold = false;   // cdb_engine_test_bounded_wait: the next batch withholds its bulk copies
   int ctasPerSm = 0;       // persistent grid: SMs x this; 0 = as many as are resident
+  int layout = CDB_LAYOUT_CELLS;   // warp-tile layout of tissues added from here on
   int numSms = 148;
-  int resident[2][CDB_MAX_REACTION_TYPES + 1] = {};   // resident CTAs per SM by [ECG][slot] (last: generic)
+  // resident CTAs per SM by [stage][ECG][slot] (last: generic)
+  int resident[4][2][CDB_MAX_REACTION_TYPES + 1] = {};
   bool anyEcg = false;     // a tissue has ECG electrodes: launch the kernels with the sensor
 
-  int grid_ctas_per_sm(int slot)
+  int grid_ctas_per_sm(int slot, int st)
   {
     if (ctasPerSm > 0) return ctasPerSm;
-    int& r = resident[anyEcg ? 1 : 0][slot < 0 ? CDB_MAX_REACTION_TYPES : slot];
-    if (r == 0) r = cfg.precision == CDB_MIXED ? resident_ctas<true>(slot, anyEcg) : resident_ctas<false>(slot, anyEcg);
+    int& r = resident[st][anyEcg ? 1 : 0][slot < 0 ? CDB_MAX_REACTION_TYPES : slot];
+    if (r == 0)
+      r = cfg.precision == CDB_MIXED ? resident_ctas<true>(slot, anyEcg, st) : resident_ctas<false>(slot, anyEcg, st);
     return r > 0 ? r : 4;
   }
 
@@ -381,7 +385,7 @@ struct Engine {
     a.nTimes = (int64_t)(dTimes.bytes / sizeof(double));
     const int slot = spec[rt] ? rt : -1;
     const unsigned grid = (unsigned)std::min<int64_t>(grid_for(a.nTiles, kWarpsPerCta),
-                                                      (int64_t)numSms * grid_ctas_per_sm(slot));
+                                                      (int64_t)numSms * grid_ctas_per_sm(slot, a.stage));
     if (cfg.precision == CDB_MIXED) launch_step<true>(slot, anyEcg, grid, st, a);
     else launch_step<false>(slot, anyEcg, grid, st, a);
     ++launches;
@@ -647,15 +651,28 @@ void build_pipe(HostTissue& h, const int64_t* gid, const std::vector<int64_t>& c
   std::vector<int> out(K, 0);
   std::vector<std::array<int64_t, CDB_MAX_REACTION_TYPES>> ends(K);
   for (int k = 0; k < CDB_MAX_REACTION_TYPES; ++k) {
+    // a tile needs the chunk holding the plane after its last cell; tiles
+    // are reordered (stably) by that chunk, so each chunk launches a prefix
+    // of its type's tiles (the kernel takes tiles in any order)
+    auto lastCell = [&](const WarpTile& tl) {
+      int64_t c = cellOf[tl.first];
+      for (int l = 1; l < tl.count; ++l) c = std::max(c, cellOf[tl.first + l]);
+      return c;
+    };
+    auto firstCell = [&](const WarpTile& tl) {
+      int64_t c = cellOf[tl.first];
+      for (int l = 1; l < tl.count; ++l) c = std::min(c, cellOf[tl.first + l]);
+      return c;
+    };
+    auto req = [&](const WarpTile& tl) { return chunk_of(std::min<int64_t>(plane(lastCell(tl)) + 1, planes - 1)); };
+    std::stable_sort(h.tiles[k].begin(), h.tiles[k].end(),
+                     [&](const WarpTile& a, const WarpTile& b) { return req(a) < req(b); });
     std::vector<int64_t> count(K, 0);
-    int prev = 0;
     for (const WarpTile& tl : h.tiles[k]) {
-      const int64_t c0 = cellOf[tl.first], c1 = cellOf[tl.first + tl.count - 1];
-      const int req = chunk_of(std::min<int64_t>(plane(c1) + 1, planes - 1));
-      if (req < prev) return;
-      prev = req;
-      ++count[req];
-      for (int ch = chunk_of(plane(c0)); ch <= chunk_of(plane(c1)); ++ch) out[ch] = std::max(out[ch], req);
+      const int r = req(tl);
+      ++count[r];
+      for (int ch = chunk_of(plane(firstCell(tl))); ch <= chunk_of(plane(lastCell(tl))); ++ch)
+        out[ch] = std::max(out[ch], r);
     }
     int64_t acc = 0;
     for (int j = 0; j < K; ++j) ends[j][k] = acc += count[j];
@@ -666,10 +683,60 @@ void build_pipe(HostTissue& h, const int64_t* gid, const std::vector<int64_t>& c
   h.pipeTiles = std::move(ends);
 }
 
+// The driver's tensor-map encoder, through the runtime's entry point (so the
+// library links only the runtime); null when the driver does not offer it.
+PFN_cuTensorMapEncodeTiled tensor_map_encoder()
+{
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled)p;
+  });
+  return fn;
+}
+
+// Stage 3's tensor maps over a volume tissue's two padded Vm blocks: FP64,
+// extents (px, ny + 2, nz + 2), row and plane strides px and pxy doubles
+// (multiples of 16 bytes: px is even), box 36 x 3 x 3 (kWinRow x 3 x 3),
+// no interleave, swizzle or multicast, zero fill outside the block.  False
+// (maps zeroed) when the strides are odd or the encoder is missing or
+// refuses.
+bool encode_vm_maps(TissueDev& d, void* vm0, void* vm1)
+{
+  std::memset(d.vmMap, 0, sizeof(d.vmMap));
+  if (d.cls != kVolume || d.px % 2 || d.pxy % 2) return false;
+  PFN_cuTensorMapEncodeTiled enc = tensor_map_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)d.px, (cuuint64_t)d.ny + 2, (cuuint64_t)d.nz + 2};
+  const cuuint64_t strides[2] = {(cuuint64_t)d.px * 8, (cuuint64_t)d.pxy * 8};
+  const cuuint32_t box[3] = {kWinRow, 3, 3};
+  const cuuint32_t elem[3] = {1, 1, 1};
+  void* base[2] = {vm0, vm1};
+  for (int k = 0; k < 2; ++k)
+    if (enc(&d.vmMap[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base[k], dims, strides, box, elem,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS) {
+      std::memset(d.vmMap, 0, sizeof(d.vmMap));
+      return false;
+    }
+  return true;
+}
+
 // Fills h.slot, h.tiles, h.nSlots and vrel (per slot: voxel offset from its
-// tile's first voxel; 0 for padding).
+// tile's first voxel; 0 for padding).  With windows (the tissue has stage
+// 3's tensor maps) row tiles are flagged kTileRow with their box origin.
+// Layout (the warp tiles' shape): CDB_LAYOUT_CELLS fills each type's blocks
+// with its cells in cell order; CDB_LAYOUT_ROWS cuts every x-row run of a
+// type (consecutive gids in one x-row) into whole 32-cell blocks from the
+// run's start, one row tile each, and packs the runs' remainders, in cell
+// order, into shared blocks (one open at a time).  Either way a type takes
+// ceil(cells / 32) blocks and every block's occupied slots are a prefix.
 cdb_status build_layout(HostTissue& h, const int64_t* gid, const uint8_t* reaction, const int* slots,
-                        const cdb_stimulus* stim, int nStim, std::vector<int32_t>& vrel)
+                        const cdb_stimulus* stim, int nStim, std::vector<int32_t>& vrel, bool windows, int layout)
 {
   const TissueDev& d = h.dev;
   const int64_t n = h.n;
@@ -683,19 +750,51 @@ cdb_status build_layout(HostTissue& h, const int64_t* gid, const uint8_t* reacti
   h.slot.resize(n);
   std::vector<int64_t> voxOf(h.nSlots, 0), cellOf(h.nSlots, -1);
   std::vector<unsigned> mask(h.nSlots / kBlk, 0u);
-  for (int64_t c = 0; c < n; ++c) {
-    const int64_t i = next[slots[reaction[c]]]++;
+  std::vector<int> fill(h.nSlots / kBlk, 0);
+  auto g = [&](int64_t c) { return gid ? gid[c] : c; };
+  auto assign = [&](int64_t c, int64_t i) {
     h.slot[c] = i;
     cellOf[i] = c;
-    const int64_t g = gid ? gid[c] : c;
-    const int x = (int)(g % h.nx);
-    const int64_t yz = g / h.nx;
+    ++fill[i / kBlk];
+    const int64_t gc = g(c);
+    const int x = (int)(gc % h.nx);
+    const int64_t yz = gc / h.nx;
     const int y = (int)(yz % h.ny), z = (int)(yz / h.ny);
     voxOf[i] = (int64_t)(x + 1) + d.px * (int64_t)(y + d.py0) + d.pxy * (int64_t)(z + d.pz0);
     for (int k = 0; k < nStim; ++k) {
       const cdb_stimulus& b = stim[k];
       if (x > b.xMin && x < b.xMax && y > b.yMin && y < b.yMax && z > b.zMin && z < b.zMax) mask[i / kBlk] |= 1u << k;
     }
+  };
+  if (layout == CDB_LAYOUT_ROWS) {
+    std::vector<std::vector<int64_t>> cellsOf(CDB_MAX_REACTION_TYPES);
+    for (int64_t c = 0; c < n; ++c) cellsOf[slots[reaction[c]]].push_back(c);
+    for (int k = 0; k < CDB_MAX_REACTION_TYPES; ++k) {
+      const std::vector<int64_t>& cs = cellsOf[k];
+      int64_t shared = -1;
+      int sfill = kBlk;
+      for (size_t a = 0; a < cs.size();) {
+        size_t e = a + 1;
+        while (e < cs.size() && g(cs[e]) == g(cs[e - 1]) + 1 && g(cs[e]) % h.nx != 0) ++e;
+        const size_t full = (e - a) / kBlk;
+        for (size_t q = 0; q < full; ++q) {
+          const int64_t blk = next[k];
+          next[k] += kBlk;
+          for (int l = 0; l < kBlk; ++l) assign(cs[a + q * kBlk + l], blk + l);
+        }
+        for (size_t r = a + full * kBlk; r < e; ++r) {
+          if (sfill == kBlk) {
+            shared = next[k];
+            next[k] += kBlk;
+            sfill = 0;
+          }
+          assign(cs[r], shared + sfill++);
+        }
+        a = e;
+      }
+    }
+  } else {
+    for (int64_t c = 0; c < n; ++c) assign(c, next[slots[reaction[c]]]++);
   }
   vrel.assign(h.nSlots, 0);
   for (auto& v : h.tiles) v.clear();
@@ -703,14 +802,23 @@ cdb_status build_layout(HostTissue& h, const int64_t* gid, const uint8_t* reacti
     for (int64_t f = start[k]; f < start[k] + count[k]; f += kBlk) {
       WarpTile tl{};
       tl.first = f;
-      tl.count = (int)std::min<int64_t>(kBlk, start[k] + count[k] - f);
+      tl.count = fill[f / kBlk];
       tl.vox0 = voxOf[f];
       tl.stimMask = mask[f / kBlk];
+      bool row = windows;
       for (int l = 0; l < tl.count; ++l) {
         const int64_t r = voxOf[f + l] - tl.vox0;
         CDB_CHECK(r >= INT32_MIN && r <= INT32_MAX, CDB_INVALID_ARG,
                   "grid too large: 32 consecutive cells of one type span more than 2^31 voxels");
         vrel[f + l] = (int32_t)r;
+        row = row && r == l;
+      }
+      tl.flags = row ? kTileRow : 0;
+      if (row) {
+        const int64_t zp = tl.vox0 / d.pxy, rem = tl.vox0 - zp * d.pxy, yp = rem / d.px, xp = rem - yp * d.px;
+        tl.wx = (int)((xp - 1) & ~int64_t(1));
+        tl.wy = (int)(yp - 1);
+        tl.wz = (int)(zp - 1);
       }
       h.tiles[k].push_back(tl);
     }
@@ -727,7 +835,7 @@ int64_t tissue_bytes(const Engine& E, const cdb_tissue_desc* t)
   int64_t count[CDB_MAX_REACTION_TYPES];
   const int64_t nSlots = count_slots(n, t->reaction, E.slots, count);
   const bool mixed = E.cfg.precision == CDB_MIXED;
-  int64_t b = 2 * vox * 8;                                                   // Vm blocks
+  int64_t b = 2 * (vox + kVmTail) * 8;                                       // Vm blocks
   b += mixed ? nSlots * (kRowsMixed64 * 8 + kRowsMixed32 * 4) : nSlots * kRows64 * 8;   // state
   b += nSlots * weight_rows(cls, mixed) * (mixed ? 4 : 8);                   // weights
   b += nSlots * (8 + 4) + n * 8 + (masked ? n * 8 : 0) + 64;                 // act, vrel, slot map, voxel
@@ -789,6 +897,7 @@ cdb_status cdb_engine_create(const cdb_engine_config* cfg, cdb_engine** out)
   // measured on the 256^3 box: bulk-copy staging is fastest for the mixed
   // step (1.02 ms against 1.10 with cp.async); FP64 keeps direct loads
   e->e.stage = cfg->precision == CDB_MIXED ? 2 : 0;
+  CDB_CUDA(cfg->precision == CDB_MIXED ? allow_step_smem<true>() : allow_step_smem<false>());
   *out = e.release();
   return CDB_OK;
 }
@@ -796,7 +905,7 @@ cdb_status cdb_engine_create(const cdb_engine_config* cfg, cdb_engine** out)
 cdb_status cdb_engine_set_tuning(cdb_engine* e, int32_t stage, int32_t ctasPerSm)
 {
   CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
-  CDB_CHECK(stage >= 0 && stage <= 2, CDB_INVALID_ARG, "stage must be 0, 1 or 2");
+  CDB_CHECK(stage >= 0 && stage <= 3, CDB_INVALID_ARG, "stage must be 0, 1, 2 or 3");
   CDB_CHECK(ctasPerSm >= 0 && ctasPerSm <= 64, CDB_INVALID_ARG, "ctasPerSm must be in [0, 64]");
   Engine& E = e->e;
   CDB_CUDA(cudaSetDevice(E.cfg.device));
@@ -807,6 +916,21 @@ cdb_status cdb_engine_set_tuning(cdb_engine* e, int32_t stage, int32_t ctasPerSm
     cudaGraphExecDestroy(E.graph);
     E.graph = nullptr;
   }
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_set_layout(cdb_engine* e, int32_t layout)
+{
+  CDB_CHECK(e, CDB_INVALID_ARG, "null engine");
+  CDB_CHECK(layout == CDB_LAYOUT_CELLS || layout == CDB_LAYOUT_ROWS, CDB_INVALID_ARG, "unknown layout");
+  e->e.layout = layout;
+  return CDB_OK;
+}
+
+cdb_status cdb_engine_get_layout(cdb_engine* e, int32_t* layout)
+{
+  CDB_CHECK(e && layout, CDB_INVALID_ARG, "null argument");
+  *layout = e->e.layout;
   return CDB_OK;
 }
 
@@ -901,14 +1025,16 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
 
   cudaStream_t s = E.stream;
   CDB_CUDA(cudaStreamSynchronize(s));
-  CDB_CUDA(h->vm0.alloc(vox * 8));
-  CDB_CUDA(h->vm1.alloc(vox * 8));
-  CDB_CUDA(cudaMemsetAsync(h->vm0.p, 0, vox * 8, s));
-  CDB_CUDA(cudaMemsetAsync(h->vm1.p, 0, vox * 8, s));
+  // (+ kVmTail zeroed doubles, read by stage 3's window rows at the block's end)
+  CDB_CUDA(h->vm0.alloc((vox + kVmTail) * 8));
+  CDB_CUDA(h->vm1.alloc((vox + kVmTail) * 8));
+  CDB_CUDA(cudaMemsetAsync(h->vm0.p, 0, (vox + kVmTail) * 8, s));
+  CDB_CUDA(cudaMemsetAsync(h->vm1.p, 0, (vox + kVmTail) * 8, s));
   // slots grouped by reaction type; AoSoA arrays cover whole 32-slot blocks
   std::vector<int32_t> vrel;
   {
-    const cdb_status ls = build_layout(*h, t->gid, t->reaction, E.slots, t->stim, t->nStim, vrel);
+    const bool windows = encode_vm_maps(d, h->vm0.p, h->vm1.p);
+    const cdb_status ls = build_layout(*h, t->gid, t->reaction, E.slots, t->stim, t->nStim, vrel, windows, E.layout);
     if (ls != CDB_OK) return ls;
   }
   const int64_t nSlots = h->nSlots;

@@ -22,6 +22,7 @@
 // with cp.async (double buffering), so the DRAM latency of those loads
 // overlaps the reaction's arithmetic.
 #pragma once
+#include <cuda.h>            // CUtensorMap (the type only: tensor maps are encoded through the runtime's driver entry point)
 #include <cuda_runtime.h>
 
 #include <cfloat>
@@ -69,22 +70,36 @@ struct TissueDev {
   double* ecgTrace;
   const void* ecgInvr;
   double hx, hy, hz;          // voxel spacing, mm
+  // Stage 3: a TMA tensor map over each padded Vm block (x, y, z extents
+  // px, ny + 2, nz + 2; box 36 x 3 x 3 doubles), for volume tissues with
+  // even strides (zero otherwise).
+  CUtensorMap vmMap[2];
 };
 
 // A warp tile: one 32-slot AoSoA block of one tissue, whose slots hold
 // cells of one reaction type (count of them, the rest are padding).  Lane l
 // works on slot first + l, whose voxel in the padded Vm block is vox0 plus
 // the slot's offset (TissueDev::vrel).  Bit k of stimMask is set when
-// stimulus k's box holds a cell of the tile.
+// stimulus k's box holds a cell of the tile.  flags: kTileRow when the
+// tile's cells are the consecutive voxels vox0, vox0 + 1, ... of one x-row
+// of a volume tissue whose padded strides are even: its stencil reads the
+// 3 x 3 rows of 34 voxels around them, which stage 3 loads into shared
+// memory as one TMA box of 36 x 3 x 3 at padded coordinates (wx, wy, wz):
+// wx = the even x at or below the first cell's x - 1, wy and wz the row's
+// y - 1 and z - 1.
+constexpr int kTileRow = 1;
 struct __align__(16) WarpTile {
   int tissue;
   int count;
   int64_t first;
   int64_t vox0;
   unsigned stimMask;
+  int flags;
+  int wx, wy, wz;
   int pad;
 };
-static_assert(sizeof(WarpTile) == 32, "tile descriptors are copied as two 16-byte chunks");
+constexpr int kDescBytes = sizeof(WarpTile);
+static_assert(kDescBytes == 48, "tile descriptors are copied as three 16-byte chunks");
 
 constexpr int kEcgRing = 1024;
 constexpr int kEcgMaxPoints = 32;
@@ -158,15 +173,48 @@ __host__ __device__ constexpr int weight_rows(int cls, bool mixed) { return mixe
 // Shared-memory staging per warp and buffer: the mixed path stages its state
 // block and its weight block (up to 18 float rows), the FP64 path its state
 // block (its weights are read directly); both stage the slots' voxel offsets.
-template <bool MIXED>
+// WGT: the mixed path's weight block is staged too (not in stage 3, whose
+// Vm window takes its shared memory; there the weights stream from global
+// memory).
+template <bool MIXED, bool WGT = true>
 __host__ __device__ constexpr int vrel_offset()
 {
-  return MIXED ? (kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4 + 18 * kBlk * 4) : kRows64 * kBlk * 8;
+  return MIXED ? (kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4 + (WGT ? 18 * kBlk * 4 : 0)) : kRows64 * kBlk * 8;
 }
-template <bool MIXED>
+template <bool MIXED, bool WGT = true>
 __host__ __device__ constexpr int stage_bytes()
 {
-  return vrel_offset<MIXED>() + kBlk * 4 + 32;   // + the next tile's descriptor
+  return vrel_offset<MIXED, WGT>() + kBlk * 4 + kDescBytes;   // + the next tile's descriptor
+}
+
+// Stage 3's Vm window of a row tile: rows (dy, dz) in {-1, 0, 1}^2, row
+// r = (dy + 1) + 3 (dz + 1), each kWinRow doubles from the even x at or
+// below the tile's first x - 1 (the TMA box, [z][y][x] in shared memory);
+// the tile's cells and their x neighbours lie within the first 35 of them.
+constexpr int kWinRow = 36;
+constexpr int kWinBytes = 9 * kWinRow * 8;
+// A TMA tensor copy's shared-memory destination must be 128-byte aligned:
+// the window region starts on a 128-byte boundary of the (128-byte aligned)
+// dynamic shared memory and each warp's window takes a multiple of 128.
+__host__ __device__ constexpr int align128(int b) { return (b + 127) / 128 * 128; }
+constexpr int kWinStride = align128(kWinBytes);
+// Padded Vm blocks carry this many zeroed doubles past their last voxel.
+constexpr int64_t kVmTail = 64;
+
+// Dynamic shared memory of a launch: per warp two staging buffers (stages
+// 1-3), three mbarriers (stages 2-3: the two buffers and the window) and,
+// for the window variant (win), one Vm window and no staged weights.
+template <bool MIXED, bool WGT>
+__host__ __device__ constexpr int win_base()
+{
+  return align128(kWarpsPerCta * (2 * stage_bytes<MIXED, WGT>() + 3 * 8));
+}
+template <bool MIXED>
+__host__ __device__ constexpr int step_smem_bytes(int stage, bool win)
+{
+  return stage == 0 ? 0
+                    : win ? win_base<MIXED, false>() + kWarpsPerCta * kWinStride
+                          : kWarpsPerCta * (2 * stage_bytes<MIXED>() + 3 * 8);
 }
 
 __device__ __forceinline__ double pulse_value(const cdb_stimulus& s, double time)
@@ -214,6 +262,33 @@ __device__ __forceinline__ double stencil32(const float* __restrict__ w, int64_t
   return (double)tmp;
 }
 
+// The same two stencils reading the neighbours from a stage-3 window: c
+// points at the cell's own voxel in the centre row, so neighbour (dx, dy,
+// dz) is c[dx + kWinRow (dy + 3 dz)], a compile-time offset.  Same
+// operands and order as the global versions, so the same results bit for
+// bit.
+__host__ __device__ constexpr int win_offset(int node)
+{
+  return node_dx(node) + kWinRow * (node_dy(node) + 3 * node_dz(node));
+}
+__device__ __forceinline__ double stencil64_win(const double* __restrict__ w, const double* c, double phi0)
+{
+  double tmp = __ldg(w) * phi0;
+#pragma unroll
+  for (int r = 1; r < class_rows(kVolume); ++r) tmp += __ldg(w + r * kBlk) * c[win_offset(class_node(kVolume, r))];
+  return tmp;
+}
+__device__ __forceinline__ double stencil32_win(const float* __restrict__ w, const double* c, double phi0)
+{
+  float tmp = 0.f;
+#pragma unroll
+  for (int r = 1; r < class_rows(kVolume); ++r) {
+    const float d = (float)(c[win_offset(class_node(kVolume, r))] - phi0);
+    tmp = fmaf(w[(r - 1) * kBlk], d, tmp);
+  }
+  return (double)tmp;
+}
+
 // State access of one cell in an AoSoA block: reads from the staged copy,
 // writes to the global block.
 struct IOBlock64 {
@@ -256,10 +331,10 @@ __device__ __forceinline__ void warp_copy(unsigned char* dst, const unsigned cha
   for (int c = lane * 16; c < bytes; c += 32 * 16) cp_async16(dst + c, src + c);
 }
 
-// Copies a 32-byte tile descriptor into shared memory (lanes 0 and 1).
+// Copies a tile descriptor into shared memory (16 bytes per lane).
 __device__ __forceinline__ void stage_desc(const WarpTile* src, WarpTile* dst, int lane)
 {
-  if (lane < 2) cp_async16((unsigned char*)dst + lane * 16, (const unsigned char*)src + lane * 16);
+  if (lane < kDescBytes / 16) cp_async16((unsigned char*)dst + lane * 16, (const unsigned char*)src + lane * 16);
 }
 
 // Copies a tile's state block (and, mixed, weight block) into buf.
@@ -393,17 +468,17 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
 // Lane 0: copies a tile's state block, weight block (mixed) and voxel
 // offsets, and the descriptor of the tile after it (when there is one),
 // into buf, all completing on bar.
-template <bool MIXED>
+template <bool MIXED, bool WGT = true>
 __device__ __forceinline__ void stage_tile_bulk(const StepArgs& a, const WarpTile& tile, unsigned char* buf,
                                                 const WarpTile* nextDesc, WarpTile* descDst, unsigned long long* bar)
 {
   const TissueDev* __restrict__ Tp = a.tissues + IndexCheck{a.nTissues, a.err}(tile.tissue);
   const int64_t b = IndexCheck{Tp->nSlots, a.err}(tile.first) / kBlk;
-  unsigned bytes = kBlk * 4 + (nextDesc ? 32u : 0u);
+  unsigned bytes = kBlk * 4 + (nextDesc ? (unsigned)kDescBytes : 0u);
   int wr = 0;
   if (MIXED) {
     bytes += kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4;
-    if (Tp->scale != 0.0) wr = weight_rows(Tp->cls, true);
+    if (WGT && Tp->scale != 0.0) wr = weight_rows(Tp->cls, true);
     bytes += wr * kBlk * 4;
   } else {
     bytes += kRows64 * kBlk * 8;
@@ -419,17 +494,133 @@ __device__ __forceinline__ void stage_tile_bulk(const StepArgs& a, const WarpTil
   } else {
     bulk_copy(buf, Tp->s64 + b * kRows64 * kBlk, kRows64 * kBlk * 8, bar);
   }
-  bulk_copy(buf + vrel_offset<MIXED>(), Tp->vrel + b * kBlk, kBlk * 4, bar);
-  if (nextDesc) bulk_copy(descDst, nextDesc, 32, bar);
+  bulk_copy(buf + vrel_offset<MIXED, WGT>(), Tp->vrel + b * kBlk, kBlk * 4, bar);
+  if (nextDesc) bulk_copy(descDst, nextDesc, kDescBytes, bar);
+}
+
+// A tile's stage-3 window: where its rows are copied and how the warp
+// waits for them (win null: the tile reads its neighbours from global
+// memory).
+struct TileWindow {
+  const double* win;            // the warp's window buffer
+  unsigned long long* bar;      // its mbarrier
+  unsigned parity;              // phase parity of this tile's copies
+};
+
+// Lane 0: loads the stencil window of row tile `tile` from Vm buffer `cur`
+// into the warp's window buffer with one TMA tensor copy (the box of 36 x 3
+// x 3 doubles at the tile's (wx, wy, wz); its x coordinate is even, so the
+// copy starts on a 16-byte boundary), completing on bar (stage 3).  Box
+// parts past the block's x extent read as zero: the stencil never uses them.
+// False, with CDB_BOUNDS_FAULT recorded and no copy issued, when the
+// destination (128 bytes), the tensor map (64 bytes) or the box's x
+// coordinate (16 bytes of doubles) is not aligned: the tile then reads its
+// neighbours from global memory.
+__device__ __forceinline__ bool stage_window(const TissueDev* __restrict__ Tp, const WarpTile* tile, int cur,
+                                             double* win, unsigned long long* bar, int* err)
+{
+  const int wx = tile->wx, wy = tile->wy, wz = tile->wz;
+  if ((smem_u32(win) & 127u) || ((unsigned long long)&Tp->vmMap[cur] & 63ull) || (wx & 1)) {
+    atomicCAS(err, 0, (int)CDB_BOUNDS_FAULT);
+    return false;
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // after the warp's reads of the last window
+  mbar_expect_tx(bar, kWinBytes);
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(win)), "l"(&Tp->vmMap[cur]), "r"(wx), "r"(wy), "r"(wz), "r"(smem_u32(bar))
+      : "memory");
+  return true;
+}
+
+// The BetterTT06 update of one cell (state through the staged block or
+// global memory); returns dVm = -Iion.  With SPEC the slot is a template
+// parameter, so every coefficient address is a compile-time constant.
+template <bool MIXED, int SLOT>
+__device__ __forceinline__ double react_cell(const StepArgs& a, const TissueDev* __restrict__ Tp, int64_t b, int pos,
+                                             const unsigned char* buf, bool staged, double phi0)
+{
+  constexpr bool SPEC = SLOT >= 0;
+  const BlockScale blk = Tp->blk;
+  const int rt = SPEC ? SLOT : a.rt;
+  const double* c64 = c_coef64 + rt * kFitPoolPerType;
+  if (MIXED) {
+    double* g64 = Tp->s64 + b * kRowsMixed64 * kBlk + pos;
+    float* g32 = Tp->s32 + b * kRowsMixed32 * kBlk + pos;
+    IOBlockMixed io{staged ? (const double*)buf + pos : g64,
+                    staged ? (const float*)(buf + kRowsMixed64 * kBlk * 8) + pos : g32, g64, g32};
+    const float* c32 = c_coef32 + rt * kFitPoolPerType;
+    if (SPEC) {
+      SpecFits fits{c64, c32};
+      return (double)tt06_step_mixed(c_scal[rt], blk, fits, (float)a.dt, phi0, io);
+    }
+    GenericFits fits{c64, c32, &c_shape[rt]};
+    return (double)tt06_step_mixed(c_scal[rt], blk, fits, (float)a.dt, phi0, io);
+  }
+  double* g64 = Tp->s64 + b * kRows64 * kBlk + pos;
+  IOBlock64 io{staged ? (const double*)buf + pos : g64, g64};
+  if (SPEC) {
+    SpecFits fits{c64, nullptr};
+    return tt06_step(c_scal[rt], blk, fits, a.dt, phi0, io);
+  }
+  GenericFits fits{c64, nullptr, &c_shape[rt]};
+  return tt06_step(c_scal[rt], blk, fits, a.dt, phi0, io);
+}
+
+// dVmD of one cell, neighbours from global memory: scale (A0 phi0 +
+// sum_k A_k phi_k) (FP64) or scale sum_k A_k (phi_k - phi0) (mixed).
+template <bool MIXED, bool WGT = true>
+__device__ __forceinline__ double stencil_global(const TissueDev* __restrict__ Tp, int64_t b, int pos,
+                                                 const unsigned char* buf, bool staged, const double* vin,
+                                                 int64_t vox, double phi0, const IndexCheck& vchk)
+{
+  const int cls = Tp->cls;
+  const int64_t px = Tp->px, pxy = Tp->pxy;
+  double acc;
+  if (MIXED) {
+    const float* w = WGT && staged ? (const float*)(buf + kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4) + pos
+                                   : (const float*)Tp->w + b * weight_rows(cls, true) * kBlk + pos;
+    acc = cls == kVolume ? stencil32<kVolume>(w, px, pxy, vin, vox, phi0, vchk)
+        : cls == kSheet ? stencil32<kSheet>(w, px, pxy, vin, vox, phi0, vchk)
+                        : stencil32<kCable>(w, px, pxy, vin, vox, phi0, vchk);
+  } else {
+    const double* w = (const double*)Tp->w + b * weight_rows(cls, false) * kBlk + pos;
+    acc = cls == kVolume ? stencil64<kVolume>(w, px, pxy, vin, vox, phi0, vchk)
+        : cls == kSheet ? stencil64<kSheet>(w, px, pxy, vin, vox, phi0, vchk)
+                        : stencil64<kCable>(w, px, pxy, vin, vox, phi0, vchk);
+  }
+  return acc * Tp->scale;
+}
+
+// Vm(t + dt) of one cell, written to vout, and its activation time
+// (ActivationTimeSensor::eval, elec/ActivationTimeSensor.cc:99-111).
+__device__ __forceinline__ double integrate_cell(const StepArgs& a, const TissueDev* __restrict__ Tp, int64_t i,
+                                                 double* vout, int64_t vox, double phi0, double dvmR, double dvmD,
+                                                 double istim, double tnext)
+{
+  const double vnew = phi0 + a.dt * (dvmR + dvmD + istim);
+  vout[vox] = vnew;
+  // Once Vm has gone above 0 the cell's activation time is set, so a cell
+  // with Vm > 0 at the start of the step already has one; only upward
+  // crossings need to read it, except in the first step after the host
+  // wrote Vm.
+  if (vnew > 0.0 && (phi0 <= 0.0 || (a.k == 0 && Tp->actAll))) {
+    double* ap = Tp->act + i;
+    if (*ap < 0.0) *ap = tnext;
+  }
+  return vnew;
 }
 
 // One tile.  With `staged` the tile's state (and mixed weights) are read
-// from buf; otherwise straight from global memory.
-template <bool MIXED, int SLOT, bool ECG>
-__device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& tile, int lane, const unsigned char* buf,
-                                          bool staged, EcgAcc& ecg, MinMaxAcc& mm)
+// from buf; otherwise straight from global memory.  WIN (stage 3): the
+// stencil runs after the reaction, on a row tile's rows copied into shared
+// memory while the reaction computed (tw.win; other tiles read global
+// memory); false when the wait for them gave up (the engine's error word
+// says CDB_TIMEOUT).
+template <bool MIXED, int SLOT, bool ECG, bool WIN>
+__device__ __forceinline__ bool step_tile(const StepArgs& a, const WarpTile& tile, int lane, const unsigned char* buf,
+                                          bool staged, const TileWindow& tw, EcgAcc& ecg, MinMaxAcc& mm)
 {
-  constexpr bool SPEC = SLOT >= 0;
   const TissueDev* __restrict__ Tp = a.tissues + IndexCheck{a.nTissues, a.err}(tile.tissue);
   const IndexCheck tchk{a.nTimes, a.err};
   const int64_t lstep = Tp->step0 + a.k;
@@ -440,7 +631,8 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
   const int l = active ? lane : 0;
   const IndexCheck schk{Tp->nSlots, a.err}, vchk{Tp->nVox, a.err};
   const int64_t i = schk(tile.first + l);
-  const int rel = staged ? ((const int*)(buf + vrel_offset<MIXED>()))[l] : Tp->vrel[i];
+  constexpr bool WGT = !WIN;     // stage 3 streams the weights from global memory
+  const int rel = staged ? ((const int*)(buf + vrel_offset<MIXED, WGT>()))[l] : Tp->vrel[i];
   const int64_t vox = vchk(tile.vox0 + rel);
   const int64_t px = Tp->px, pxy = Tp->pxy;
   // iStim = 0, then the stimuli whose boxes hold a cell of the tile, in order
@@ -461,80 +653,47 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
       }
     }
   }
+  const int64_t b = i / kBlk;
+  const int pos = (int)(i - b * kBlk);
+  const int cur = (Tp->parity + a.k) & 1;
+  const double* __restrict__ vin = Tp->vm[cur];
+  double* __restrict__ vout = Tp->vm[cur ^ 1];
   double vnew = 0.0;
   double ecgSrc = 0.0;        // the cell's dVmD, the ECG's source term
-  if (active) {
-    const int cur = (Tp->parity + a.k) & 1;
-    const double* __restrict__ vin = Tp->vm[cur];
-    double* __restrict__ vout = Tp->vm[cur ^ 1];
-    const double scale = Tp->scale;
-    const int cls = Tp->cls;
-    const BlockScale blk = Tp->blk;
-    const int64_t b = i / kBlk;
-    const int pos = (int)(i - b * kBlk);
-    const double phi0 = vin[vox];
-
-    double dvmD = 0.0;
-    if (scale != 0.0) {
-      double acc;
-      if (MIXED) {
-        const int wr = weight_rows(cls, true);
-        const float* w = staged ? (const float*)(buf + kRowsMixed64 * kBlk * 8 + kRowsMixed32 * kBlk * 4) + pos
-                                : (const float*)Tp->w + b * wr * kBlk + pos;
-        acc = cls == kVolume ? stencil32<kVolume>(w, px, pxy, vin, vox, phi0, vchk)
-            : cls == kSheet ? stencil32<kSheet>(w, px, pxy, vin, vox, phi0, vchk)
-                            : stencil32<kCable>(w, px, pxy, vin, vox, phi0, vchk);
-      } else {
-        const int wr = weight_rows(cls, false);
-        const double* w = (const double*)Tp->w + b * wr * kBlk + pos;
-        acc = cls == kVolume ? stencil64<kVolume>(w, px, pxy, vin, vox, phi0, vchk)
-            : cls == kSheet ? stencil64<kSheet>(w, px, pxy, vin, vox, phi0, vchk)
-                            : stencil64<kCable>(w, px, pxy, vin, vox, phi0, vchk);
+  if (!WIN) {
+    if (active) {
+      const double phi0 = vin[vox];
+      const double dvmD = Tp->scale != 0.0 ? stencil_global<MIXED>(Tp, b, pos, buf, staged, vin, vox, phi0, vchk) : 0.0;
+      ecgSrc = dvmD;
+      const double dvmR = react_cell<MIXED, SLOT>(a, Tp, b, pos, buf, staged, phi0);
+      vnew = integrate_cell(a, Tp, i, vout, vox, phi0, dvmR, dvmD, istim, tnext);
+    }
+  } else {
+    double phi0 = 0.0, dvmR = 0.0, dvmD = 0.0;
+    if (active) {
+      phi0 = vin[vox];
+      dvmR = react_cell<MIXED, SLOT>(a, Tp, b, pos, buf, staged, phi0);
+    }
+    if (tw.win) {
+      // the row tile's window, copied while the reaction computed (every lane waits)
+      if (!__all_sync(0xffffffffu, mbar_wait(tw.bar, tw.parity))) {
+        if (lane == 0) atomicExch(a.err, (int)CDB_TIMEOUT);
+        mbar_wait(tw.bar, tw.parity);      // let its copies land before the warp leaves
+        return false;
       }
-      dvmD = acc * scale;
+      if (active && Tp->scale != 0.0) {
+        const double* c = tw.win + 4 * kWinRow + (int)((tile.vox0 - 1) & 1) + 1 + l;
+        if (MIXED)
+          dvmD = stencil32_win((const float*)Tp->w + b * weight_rows(kVolume, true) * kBlk + pos, c, phi0);
+        else
+          dvmD = stencil64_win((const double*)Tp->w + b * weight_rows(kVolume, false) * kBlk + pos, c, phi0);
+        dvmD *= Tp->scale;
+      }
+    } else if (active && Tp->scale != 0.0) {
+      dvmD = stencil_global<MIXED, WGT>(Tp, b, pos, buf, staged, vin, vox, phi0, vchk);
     }
     ecgSrc = dvmD;
-
-    // With SPEC the slot is a template parameter, so every coefficient
-    // address is a compile-time constant.
-    const int rt = SPEC ? SLOT : a.rt;
-    const double* c64 = c_coef64 + rt * kFitPoolPerType;
-    double dvmR;
-    if (MIXED) {
-      double* g64 = Tp->s64 + b * kRowsMixed64 * kBlk + pos;
-      float* g32 = Tp->s32 + b * kRowsMixed32 * kBlk + pos;
-      IOBlockMixed io{staged ? (const double*)buf + pos : g64,
-                      staged ? (const float*)(buf + kRowsMixed64 * kBlk * 8) + pos : g32, g64, g32};
-      const float* c32 = c_coef32 + rt * kFitPoolPerType;
-      if (SPEC) {
-        SpecFits fits{c64, c32};
-        dvmR = (double)tt06_step_mixed(c_scal[rt], blk, fits, (float)a.dt, phi0, io);
-      } else {
-        GenericFits fits{c64, c32, &c_shape[rt]};
-        dvmR = (double)tt06_step_mixed(c_scal[rt], blk, fits, (float)a.dt, phi0, io);
-      }
-    } else {
-      double* g64 = Tp->s64 + b * kRows64 * kBlk + pos;
-      IOBlock64 io{staged ? (const double*)buf + pos : g64, g64};
-      if (SPEC) {
-        SpecFits fits{c64, nullptr};
-        dvmR = tt06_step(c_scal[rt], blk, fits, a.dt, phi0, io);
-      } else {
-        GenericFits fits{c64, nullptr, &c_shape[rt]};
-        dvmR = tt06_step(c_scal[rt], blk, fits, a.dt, phi0, io);
-      }
-    }
-
-    vnew = phi0 + a.dt * (dvmR + dvmD + istim);
-    vout[vox] = vnew;
-    // Once Vm has gone above 0 the cell's activation time is set, so a cell
-    // with Vm > 0 at the start of the step already has one; only upward
-    // crossings need to read it, except in the first step after the host
-    // wrote Vm.
-    if (vnew > 0.0 && (phi0 <= 0.0 || (a.k == 0 && Tp->actAll))) {
-      double* ap = Tp->act + i;
-      if (*ap < 0.0) *ap = tnext;
-    }
+    if (active) vnew = integrate_cell(a, Tp, i, vout, vox, phi0, dvmR, dvmD, istim, tnext);
   }
   if (a.minmax) {
     if (mm.tissue != tile.tissue) {
@@ -566,7 +725,7 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
       ecg.tissue = tile.tissue;
       ecg.entry = entry;
     }
-    const int64_t b = i / kBlk, at = b * ecgN * kBlk + (i - b * kBlk);
+    const int64_t at = b * ecgN * kBlk + pos;
     const double* __restrict__ inv64 = (const double*)Tp->ecgInvr + at;
     const float* __restrict__ inv32 = (const float*)Tp->ecgInvr + at;
     for (int g = 0; g < ecgN; g += 8) {
@@ -583,6 +742,7 @@ __device__ __forceinline__ void step_tile(const StepArgs& a, const WarpTile& til
     if (tile.first == 0 && lane < ecgN)
       Tp->ecgTrace[(int64_t)((entry + 1) % kEcgRing) * ecgN + lane] = 0.0;
   }
+  return true;
 }
 
 // Resident CTAs per SM the register budget aims at: 4 for FP64 (16 warps,
@@ -601,11 +761,15 @@ constexpr int min_ctas() { return MIXED ? 5 : CDB_FP64_MIN_CTAS; }
 // SLOT >= 0: the launch's reaction type is constant-memory slot SLOT and its
 // fits have the compiled shapes (fit_shapes.h); SLOT < 0: any slot (a.rt)
 // with run-time shapes.
-template <bool MIXED, int SLOT, bool ECG>
+// WIN: the stage-3 variant (Vm windows of row tiles; only stage-3 launches
+// of the compiled slots without ECG use it).
+template <bool MIXED, int SLOT, bool ECG, bool WIN>
 __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(StepArgs a)
 {
-  constexpr int kBuf = stage_bytes<MIXED>();
-  __shared__ __align__(16) unsigned char smem[kWarpsPerCta * 2 * kBuf + kWarpsPerCta * 2 * 8];
+  constexpr bool WGT = !WIN;
+  constexpr int kBuf = stage_bytes<MIXED, WGT>();
+  // dynamic: step_smem_bytes<MIXED>(a.stage, WIN) bytes (none for stage 0)
+  extern __shared__ __align__(128) unsigned char smem[];
   __shared__ double ecgSmem[ECG ? kWarpsPerCta * 32 : 1];   // each warp's ECG sums
   const int lane = threadIdx.x & 31;
   const int warpInCta = threadIdx.x >> 5;
@@ -617,7 +781,8 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
   unsigned char* mine = smem + warpInCta * 2 * kBuf;
   const int stride = gridDim.x * kWarpsPerCta;
   int t = blockIdx.x * kWarpsPerCta + warpInCta;
-  if (!a.stage) {
+  const TileWindow noWin{nullptr, nullptr, 0};
+  if (!WIN && !a.stage) {
     // the next tile's descriptor is in flight while this tile computes
     WarpTile cur, nxt;
     EcgAcc ecg{ecgMine, -1, 0};
@@ -625,24 +790,29 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
     if (t < a.nTiles) cur = a.tiles[t];
     for (; t < a.nTiles; t += stride) {
       if (t + stride < a.nTiles) nxt = a.tiles[t + stride];
-      step_tile<MIXED, SLOT, ECG>(a, cur, lane, nullptr, false, ecg, mm);
+      step_tile<MIXED, SLOT, ECG, false>(a, cur, lane, nullptr, false, noWin, ecg, mm);
       cur = nxt;
     }
     if (ECG) ecg_flush(a, ecg, lane);
     if (a.minmax) minmax_flush(a, mm, lane);
     return;
   }
-  if (a.stage == 2) {
+  if (WIN || a.stage >= 2) {
     // Bulk copies: lane 0 issues, for tile t + stride, cp.async.bulk copies
     // of its contiguous blocks (and of the descriptor after it) into the
     // other buffer while the warp computes tile t; every lane waits on the
-    // buffer's mbarrier, phase (iteration / 2) & 1.
-    unsigned long long* bars = (unsigned long long*)(smem + kWarpsPerCta * 2 * kBuf) + warpInCta * 2;
-    WarpTile* const desc0 = (WarpTile*)(mine + vrel_offset<MIXED>() + kBlk * 4);
-    WarpTile* const desc1 = (WarpTile*)(mine + kBuf + vrel_offset<MIXED>() + kBlk * 4);
+    // buffer's mbarrier, phase (iteration / 2) & 1.  Stage 3 also copies a
+    // row tile's nine stencil rows into the warp's window at the start of
+    // its iteration (third mbarrier, phase = windows so far & 1), read after
+    // the reaction.
+    unsigned long long* bars = (unsigned long long*)(smem + kWarpsPerCta * 2 * kBuf) + warpInCta * 3;
+    double* const win = WIN ? (double*)(smem + win_base<MIXED, WGT>() + warpInCta * kWinStride) : nullptr;
+    WarpTile* const desc0 = (WarpTile*)(mine + vrel_offset<MIXED, WGT>() + kBlk * 4);
+    WarpTile* const desc1 = (WarpTile*)(mine + kBuf + vrel_offset<MIXED, WGT>() + kBlk * 4);
     if (lane == 0) {
       mbar_init(bars, 1);
       mbar_init(bars + 1, 1);
+      mbar_init(bars + 2, 1);
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
@@ -650,7 +820,8 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
     MinMaxAcc mm{__longlong_as_double(0x7ff0000000000000ll), -__longlong_as_double(0x7ff0000000000000ll), -1};
     WarpTile cur = t < a.nTiles ? a.tiles[t] : WarpTile{};
     if (t < a.nTiles && lane == 0)
-      stage_tile_bulk<MIXED>(a, cur, mine, t + stride < a.nTiles ? a.tiles + t + stride : nullptr, desc0, bars);
+      stage_tile_bulk<MIXED, WGT>(a, cur, mine, t + stride < a.nTiles ? a.tiles + t + stride : nullptr, desc0, bars);
+    unsigned windows = 0;
     for (int it = 0; t < a.nTiles; ++it, t += stride) {
       const int tn = t + stride;
       const int bi = it & 1;
@@ -659,19 +830,40 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
         mbar_wait(bars + bi, (it >> 1) & 1);    // let its copies land before the warp leaves
         return;
       }
-      __syncwarp();           // every lane is past the wait and done with the other buffer
+      __syncwarp();           // every lane is past the wait and done with the other buffer (and the window)
       const WarpTile nxt = tn < a.nTiles ? *(bi ? desc1 : desc0) : WarpTile{};
-      if (tn < a.nTiles && lane == 0 && !a.withhold)
-        stage_tile_bulk<MIXED>(a, nxt, mine + (bi ^ 1) * kBuf,
+      const bool next = tn < a.nTiles && !a.withhold;
+      TileWindow tw = noWin;
+      if (WIN && (cur.flags & kTileRow)) {
+        // the window's box origin, from this tile's descriptor: in global
+        // memory for the first tile, else still in the slot the next copy
+        // overwrites (so before that copy is issued)
+        bool issued = false;
+        if (lane == 0) {
+          const TissueDev* __restrict__ Tp = a.tissues + IndexCheck{a.nTissues, a.err}(cur.tissue);
+          issued = stage_window(Tp, it == 0 ? a.tiles + t : (bi ? desc0 : desc1), (Tp->parity + a.k) & 1, win,
+                                bars + 2, a.err);
+        }
+        if (__shfl_sync(0xffffffffu, issued, 0)) {
+          tw = TileWindow{win, bars + 2, windows & 1u};
+          ++windows;
+        }
+      }
+      if (next && lane == 0)
+        stage_tile_bulk<MIXED, WGT>(a, nxt, mine + (bi ^ 1) * kBuf,
                                tn + stride < a.nTiles ? a.tiles + tn + stride : nullptr, bi ? desc0 : desc1,
                                bars + (bi ^ 1));
-      step_tile<MIXED, SLOT, ECG>(a, cur, lane, mine + bi * kBuf, true, ecg, mm);
+      if (!step_tile<MIXED, SLOT, ECG, WIN>(a, cur, lane, mine + bi * kBuf, true, tw, ecg, mm)) {
+        if (next) mbar_wait(bars + (bi ^ 1), ((it + 1) >> 1) & 1);   // the next tile's copies, in flight
+        return;
+      }
       cur = nxt;
     }
     if (ECG) ecg_flush(a, ecg, lane);
     if (a.minmax) minmax_flush(a, mm, lane);
     return;
   }
+  if (WIN) return;
   // Buffer i holds tile t's inputs and the descriptor of tile t + stride,
   // copied together one iteration ahead.
   WarpTile* desc0 = (WarpTile*)(mine + vrel_offset<MIXED>() + kBlk * 4);
@@ -697,7 +889,7 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
       if (tn + stride < a.nTiles) stage_desc(a.tiles + tn + stride, nextDesc, lane);
     }
     cp_async_commit();
-    step_tile<MIXED, SLOT, ECG>(a, cur, lane, mine + (it & 1) * kBuf, true, ecg, mm);
+    step_tile<MIXED, SLOT, ECG, false>(a, cur, lane, mine + (it & 1) * kBuf, true, noWin, ecg, mm);
     cur = nxt;
   }
   cp_async_wait_all();
@@ -707,41 +899,71 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
 
 // The compiled kernel of a slot when the type has the compiled fit shapes
 // (slot >= 0), else the generic kernel; with the ECG sensor compiled in or
-// out (only launches that hold a tissue with electrodes pay for it).
-template <bool MIXED, bool ECG>
+// out (only launches that hold a tissue with electrodes pay for it); for
+// stage 3, the compiled slots without ECG run the window variant (the
+// others run stage 3 as stage 2).
+template <bool MIXED, bool ECG, bool WIN>
 inline void (*step_kernel_of(int slot))(StepArgs)
 {
   static_assert(CDB_MAX_REACTION_TYPES == 6, "one compiled kernel per slot");
   switch (slot) {
-    case 0: return fused_step_kernel<MIXED, 0, ECG>;
-    case 1: return fused_step_kernel<MIXED, 1, ECG>;
-    case 2: return fused_step_kernel<MIXED, 2, ECG>;
-    case 3: return fused_step_kernel<MIXED, 3, ECG>;
-    case 4: return fused_step_kernel<MIXED, 4, ECG>;
-    case 5: return fused_step_kernel<MIXED, 5, ECG>;
-    default: return fused_step_kernel<MIXED, -1, ECG>;
+    case 0: return fused_step_kernel<MIXED, 0, ECG, WIN>;
+    case 1: return fused_step_kernel<MIXED, 1, ECG, WIN>;
+    case 2: return fused_step_kernel<MIXED, 2, ECG, WIN>;
+    case 3: return fused_step_kernel<MIXED, 3, ECG, WIN>;
+    case 4: return fused_step_kernel<MIXED, 4, ECG, WIN>;
+    case 5: return fused_step_kernel<MIXED, 5, ECG, WIN>;
+    default: return fused_step_kernel<MIXED, -1, ECG, false>;
   }
 }
 
+// Whether a launch runs the window variant.
+inline bool step_uses_window(int slot, bool ecg, int stage) { return stage == 3 && !ecg && slot >= 0; }
+
 template <bool MIXED>
-inline void (*step_kernel_for(int slot, bool ecg))(StepArgs)
+inline void (*step_kernel_for(int slot, bool ecg, int stage))(StepArgs)
 {
-  return ecg ? step_kernel_of<MIXED, true>(slot) : step_kernel_of<MIXED, false>(slot);
+  if (ecg) return step_kernel_of<MIXED, true, false>(slot);
+  return stage == 3 ? step_kernel_of<MIXED, false, true>(slot) : step_kernel_of<MIXED, false, false>(slot);
 }
 
-// One step of one reaction type.
+template <bool MIXED>
+inline int step_launch_smem(int slot, bool ecg, int stage)
+{
+  return step_smem_bytes<MIXED>(stage, step_uses_window(slot, ecg, stage));
+}
+
+// One step of one reaction type (dynamic shared memory for a.stage).
 template <bool MIXED>
 inline void launch_step(int slot, bool ecg, unsigned grid, cudaStream_t stream, const StepArgs& a)
 {
-  step_kernel_for<MIXED>(slot, ecg)<<<grid, kCta, 0, stream>>>(a);
+  step_kernel_for<MIXED>(slot, ecg, a.stage)<<<grid, kCta, step_launch_smem<MIXED>(slot, ecg, a.stage), stream>>>(a);
 }
 
-// CTAs of a slot's kernel that are resident on one SM at once (0 on error).
+// Lets every step kernel of a precision take stage 3's dynamic shared
+// memory (above the default 48 KB limit); once per device, before any
+// launch or capture.
 template <bool MIXED>
-inline int resident_ctas(int slot, bool ecg)
+inline cudaError_t allow_step_smem()
+{
+  for (int slot = -1; slot < CDB_MAX_REACTION_TYPES; ++slot)
+    for (int v = 0; v < 3; ++v) {        // ECG, no ECG, window variant
+      const cudaError_t e = cudaFuncSetAttribute(step_kernel_for<MIXED>(slot, v == 0, v == 2 ? 3 : 2),
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 step_launch_smem<MIXED>(slot, v == 0, v == 2 ? 3 : 2));
+      if (e != cudaSuccess) return e;
+    }
+  return cudaSuccess;
+}
+
+// CTAs of a slot's kernel that are resident on one SM at once with the
+// stage's shared memory (0 on error).
+template <bool MIXED>
+inline int resident_ctas(int slot, bool ecg, int stage)
 {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel_for<MIXED>(slot, ecg), kCta, 0) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel_for<MIXED>(slot, ecg, stage), kCta,
+                                                    step_launch_smem<MIXED>(slot, ecg, stage)) != cudaSuccess)
     return 0;
   return n;
 }

@@ -179,8 +179,11 @@ cdb_status cdb_diff6_destroy(cdb_diff6* d);
  * rejected with CDB_INVALID_ARG.  The call allocates nothing: no cudaMalloc,
  * no cudaFree.  Its first call on a device looks up that array's device
  * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  Every call shares the one array and clears it first; calls that
- * overlap on the GPU (other streams, other threads) race on it. */
+ * capture, and do not cudaDeviceReset that device afterwards (the address
+ * is kept for the life of the process).  Every call shares the one array
+ * and clears it first; calls that overlap on the GPU (other streams, other
+ * threads) race on it.  The calling thread's current device is the same on
+ * return as on entry. */
 cdb_status cdb_fgr_calc_static(int device, int32_t nx, int32_t ny, int32_t nz, const double* weights19,
                                const double* Vm, double* dVm, double diffusionScale, void* stream);
 
@@ -300,13 +303,28 @@ cdb_status cdb_diag_fit_forms(const cdb_fit fits[CDB_NUM_FITS], int32_t poolSize
 /* Launch tuning of the step kernel (no counterpart in the reference):
  * stage 1 = each warp copies its next tile's state (mixed: and weights)
  * into shared memory with cp.async while it computes the current one, 2 =
- * the same with bulk (TMA) copies completing on an mbarrier, 0 = direct
- * loads; ctasPerSm sizes the persistent grid (SMs x ctasPerSm CTAs
- * of 128 threads), 0 = as many CTAs as are resident on an SM at once.
- * Defaults: stage 2 for CDB_MIXED, 0 for CDB_FP64, ctasPerSm 0;
+ * the same with bulk (TMA) copies completing on an mbarrier, 3 = stage 2
+ * plus the Vm tile and halo of every row tile (32 consecutive voxels of one
+ * x-row of a volume tissue with even padded strides): its nine stencil rows
+ * are bulk-copied into shared memory while the reaction computes and the
+ * stencil reads them there, 0 = direct loads; ctasPerSm sizes the
+ * persistent grid (SMs x ctasPerSm CTAs of 128 threads), 0 = as many CTAs as
+ * are resident on an SM at once.  All stages give the same results bit for
+ * bit.  Defaults: stage 2 for CDB_MIXED, 0 for CDB_FP64, ctasPerSm 0;
  * cardioid_b200.autotune picks them by timing. */
 cdb_status cdb_engine_set_tuning(cdb_engine* e, int32_t stage, int32_t ctasPerSm);
 cdb_status cdb_engine_get_tuning(cdb_engine* e, int32_t* stage, int32_t* ctasPerSm);
+
+/* Warp-tile layout of the tissues added after the call (no counterpart in
+ * the reference): CDB_LAYOUT_CELLS (default) fills each reaction type's
+ * 32-slot blocks with its cells in cell order; CDB_LAYOUT_ROWS cuts every
+ * x-row run of a type into whole 32-cell row tiles (stage 3 stages their
+ * Vm tile and halo) and packs the runs' remainders into shared blocks.  Same
+ * results bit for bit; cardioid_b200.autotune picks it by timing. */
+#define CDB_LAYOUT_CELLS 0
+#define CDB_LAYOUT_ROWS 1
+cdb_status cdb_engine_set_layout(cdb_engine* e, int32_t layout);
+cdb_status cdb_engine_get_layout(cdb_engine* e, int32_t* layout);
 
 /* Kernels launched by this engine since creation. */
 cdb_status cdb_engine_launch_count(cdb_engine* e, int64_t* launches);

@@ -25,15 +25,24 @@ def masked(nx, ny, nz, seed=3):
                          full.sigma[keep], full.vm0[keep], full.stimuli)
 
 
+def rows(nx, ny, nz):
+    """One cell type, x-rows of whole warp tiles: stage 3's Vm windows, the
+    last one reading past the padded block's last voxel."""
+    t = tissue.box(nx, ny, nz)
+    t.cell_type[:] = 100
+    return t
+
+
 def tissues():
     return {"box": tissue.box(9, 8, 7), "cable": tissue.box(40, 1, 1), "sheet": tissue.box(12, 9, 1),
-            "masked": masked(16, 14, 12), "one": tissue.box(1, 1, 1), "ragged": tissue.box(33, 1, 1)}
+            "masked": masked(16, 14, 12), "one": tissue.box(1, 1, 1), "ragged": tissue.box(33, 1, 1),
+            "rows": rows(64, 5, 4)}
 
 
 def run(out):
     res = {}
     for prec in ("fp64", "mixed"):
-        for stage in (0, 1, 2):
+        for stage in (0, 1, 2, 3):
             # every tissue alone and all of them in one engine (one launch per type)
             ts = tissues()
             with engine.Engine(DT, precision=prec) as e:

@@ -3,7 +3,7 @@ slot and voxel index the step kernel uses is checked, and one out of range
 is recorded as CDB_BOUNDS_FAULT instead of being accessed; the stand-in for
 a memory checker where compute-sanitizer is closed) on small and edge-case
 tissues: boxes, cables, sheets, a masked tissue, one cell, ragged type
-groups, all of them in one engine, the ECG sensor, the three staging modes
+groups, row tiles, all of them in one engine, the ECG sensor, the four staging modes
 and the chunked host step, FP64 and mixed.  Each library runs in its own
 process (tests/bounds_cases.py); the checked run must report no fault
 (cdb_engine_sync) and give the same results as the normal build (bit for

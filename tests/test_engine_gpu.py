@@ -310,24 +310,84 @@ def test_full_size_box_mixed_vs_fp64_and_repeatable(cdb_lib):
     assert np.abs(a[both] - m[both]).max() <= ACT_TOL_MIXED
 
 
+def _rows_box(nx, ny, nz, seed):
+    """A box of one cell type whose x-rows are whole warp tiles (nx a
+    multiple of 32, even padded strides): every tile is a row tile, which
+    stage 3 stages through the Vm window; the last one ends at the padded
+    block's last voxels."""
+    t = tissue.box(nx, ny, nz, seed=seed)
+    t.cell_type[:] = 101
+    return t
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_staging_modes_agree(cdb_lib, fits002, precision):
-    """Direct loads (0), per-lane cp.async staging (1) and bulk-copy staging
-    on mbarriers (2) compute the same bits, on a mix of tissue classes and
-    with several tiles per warp (small grid)."""
-    ts = [tissue.box(40, 33, 9, seed=8), tissue.box(300, 1, 1, seed=9), _masked(13, 12, 11, seed=10)]
+    """Direct loads (0), per-lane cp.async staging (1), bulk-copy staging on
+    mbarriers (2) and bulk-copy staging with the Vm tile and halo of row
+    tiles in shared memory (3) compute the same bits, on a mix of tissue
+    classes (row tiles, multi-row tiles, a cable, a masked tissue) and with
+    several tiles per warp (small grid)."""
+    ts = [tissue.box(40, 33, 9, seed=8), tissue.box(300, 1, 1, seed=9), _masked(13, 12, 11, seed=10),
+          _rows_box(64, 6, 5, seed=11)]
     out = {}
-    for stage in (0, 1, 2):
+    for stage in (0, 1, 2, 3):
         with _engine(fits002, precision=precision) as e:
             e.set_tuning(stage, 1)
             ids = [e.add_tissue(t, _reaction_ids(t)) for t in ts]
             e.step(60)
             e.sync()
             out[stage] = [(e.read_vm(i), e.read_states(i), e.read_activation(i)) for i in ids]
-    for stage in (1, 2):
+    for stage in (1, 2, 3):
         for a, b in zip(out[0], out[stage]):
             for x, y in zip(a, b):
                 np.testing.assert_array_equal(x, y)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tile_layouts_agree(cdb_lib, fits002, precision):
+    """The two warp-tile layouts (cells in cell order; x-row runs cut into
+    whole row tiles with packed remainders) give the same bits, with bulk
+    staging (2) and with the Vm windows of row tiles (3), on a box whose
+    type slabs are 25 / 35 / 40 cells wide along x, a masked tissue and a
+    cable, in one engine."""
+    ts = [tissue.box(100, 7, 6, seed=12), _masked(70, 6, 5, seed=13), tissue.box(150, 1, 1, seed=14)]
+    out = {}
+    for layout in ("cells", "rows"):
+        for stage in (2, 3):
+            with _engine(fits002, precision=precision) as e:
+                e.set_tuning(stage, 1)
+                e.set_layout(layout)
+                assert e.get_layout() == layout
+                ids = [e.add_tissue(t, _reaction_ids(t)) for t in ts]
+                e.step(40)
+                e.sync()
+                out[layout, stage] = [(e.read_vm(i), e.read_states(i), e.read_activation(i)) for i in ids]
+    for key in out:
+        for a, b in zip(out["cells", 2], out[key]):
+            for x, y in zip(a, b):
+                np.testing.assert_array_equal(x, y, err_msg=str(key))
+
+
+def test_rows_layout_host_step_matches_device_steps(cdb_lib, fits002):
+    """The chunked host step on a rows-layout tissue (tiles reordered by the
+    chunk they need) matches steps on device-resident Vm bit for bit."""
+    t = tissue.box(96, 40, 36, seed=15)
+    res = {}
+    for mode in ("device", "host"):
+        with _engine(fits002, precision="mixed") as e:
+            e.set_layout("rows")
+            tid = e.add_tissue(t, _reaction_ids(t))
+            if mode == "device":
+                e.step(12)
+                res[mode] = e.read_vm(tid)
+            else:
+                vm = np.ascontiguousarray(t.vm0)
+                o = np.empty_like(vm)
+                for _ in range(12):
+                    e.step_host(tid, vm, o)
+                    vm, o = o, vm
+                res[mode] = vm
+    np.testing.assert_array_equal(res["device"], res["host"])
 
 
 def _cube_in(n_box, off, side=8, seed=5):
