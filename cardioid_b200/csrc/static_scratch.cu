@@ -15,6 +15,12 @@
 // clears the whole block it uses before filling it.  Two calls whose
 // kernels overlap on the GPU (different streams, or different host threads)
 // race on the block: a caller serialises them, e.g. on one stream.
+//
+// The array's device address is looked up on the first call on each device
+// and kept: a cudaDeviceReset on that device after the first call (which
+// unloads the module, so the array may come back elsewhere) is not
+// supported.  The call leaves the calling thread's current device as it
+// found it.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -80,6 +86,26 @@ __global__ void static_stencil_kernel(const double* __restrict__ w19, const doub
   dVm[i] = tmp * scale;
 }
 
+// Makes `device` current for the call and restores the caller's current
+// device when the call returns (the entry point runs inside other
+// frameworks' code, whose device choice it must not change).
+struct DeviceScope {
+  int prev = -1;
+  cudaError_t enter(int device)
+  {
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) {
+      prev = -1;
+      return e;
+    }
+    return prev == device ? cudaSuccess : cudaSetDevice(device);
+  }
+  ~DeviceScope()
+  {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 }  // namespace
 }  // namespace cdb
 
@@ -95,7 +121,8 @@ extern "C" cdb_status cdb_fgr_calc_static(int device, int32_t nx, int32_t ny, in
   CDB_CHECK(nvox <= kStaticVoxels, CDB_INVALID_ARG,
             "box too large for cdb_fgr_calc_static: (nx+2)(ny+2)(nz+2) = " + std::to_string(nvox) +
                 " voxels exceeds the static block of " + std::to_string(kStaticVoxels) + " voxels (16 MiB)");
-  CDB_CUDA(cudaSetDevice(device));
+  DeviceScope scope;
+  CDB_CUDA(scope.enter(device));
   double* blk = nullptr;
   CDB_CUDA(static_block(device, &blk));
   const int64_t n = (int64_t)nx * ny * nz;

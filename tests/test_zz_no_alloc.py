@@ -1,8 +1,10 @@
 """cdb_fgr_calc_static, the FGR stencil for callers that cannot allocate
 device memory (it keeps its padded Vm block in a static device array),
 against the allocating entry points cdb_fgr_create / _update_local_voltage /
-_calc on the same box, for two calls in a row with different voltages (the
-second call must not see the first call's block).
+_calc, for two calls in a row: first on a larger box, then on a smaller one,
+so the first call's values sit where the second call's halo is (the second
+call must clear them).  A warmed-up call leaves the device's free memory
+unchanged and the calling thread's current device as it was.
 
 This file is collected last so that a run stopping at the first failure has
 already run every other test."""
@@ -23,24 +25,51 @@ def _static_calc(lib, t, w19_dev, vm_dev, out_dev, stream):
                                    t.diffusion_scale, ctypes.c_void_p(stream))
 
 
+def _case(t, scale, seed):
+    """Weights (19 rows of n on the device), a voltage and the allocating
+    path's dVm for box t."""
+    import torch
+    ref = plugins.FGRDiffusion(t)
+    w19 = torch.from_numpy(np.ascontiguousarray(ref.weights().T)).cuda()
+    rng = np.random.default_rng(seed)
+    vm = torch.from_numpy(t.vm0 + rng.uniform(-20.0, 60.0, t.n) * scale).cuda()
+    want = torch.empty_like(vm)
+    ref.updateLocalVoltage(vm)
+    ref.calc(want)
+    torch.cuda.synchronize()
+    return w19, vm, want.cpu().numpy()
+
+
 def test_static_scratch_stencil_matches_allocating_path_twice(cdb_lib):
     import torch
-    t = tissue.box(23, 17, 11, seed=9)
-    ref = plugins.FGRDiffusion(t)
-    w19 = torch.from_numpy(np.ascontiguousarray(ref.weights().T)).cuda()   # 19 rows of n
     stream = torch.cuda.current_stream().cuda_stream
-    rng = np.random.default_rng(4)
-    for call in range(2):
-        vm = torch.from_numpy(t.vm0 + rng.uniform(-20.0, 60.0, t.n) * (call + 1)).cuda()
-        want = torch.empty_like(vm)
-        ref.updateLocalVoltage(vm)
-        ref.calc(want)
+    for call, t in enumerate((tissue.box(23, 17, 11, seed=9), tissue.box(11, 9, 7, seed=10))):
+        w19, vm, want = _case(t, call + 1, 4 + call)
         got = torch.full_like(vm, float("nan"))
         _lib.check(_static_calc(cdb_lib, t, w19, vm, got, stream))
         torch.cuda.synchronize()
-        w, g = want.cpu().numpy(), got.cpu().numpy()
+        g = got.cpu().numpy()
         assert np.isfinite(g).all()
-        assert np.abs(g - w).max() <= REL_TOL * np.abs(w).max(), call
+        assert np.abs(g - want).max() <= REL_TOL * np.abs(want).max(), call
+
+
+def test_static_scratch_allocates_nothing(cdb_lib):
+    """After a first call (which may load the library's module on this
+    device), another call leaves the device's free memory unchanged."""
+    import torch
+    t = tissue.box(15, 13, 9, seed=11)
+    w19, vm, want = _case(t, 1, 12)
+    got = torch.empty_like(vm)
+    stream = torch.cuda.current_stream().cuda_stream
+    _lib.check(_static_calc(cdb_lib, t, w19, vm, got, stream))
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    _lib.check(_static_calc(cdb_lib, t, w19, vm, got, stream))
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.cuda.current_device() == 0
+    assert np.abs(got.cpu().numpy() - want).max() <= REL_TOL * np.abs(want).max()
 
 
 def test_static_scratch_rejects_boxes_beyond_its_block(cdb_lib):
