@@ -117,6 +117,31 @@ def test_port_bit_exact_vs_reference_build(oracle_port, fits002, shape):
 
 
 @pytest.mark.skipif(not _ref_built(), reason="oracle/_ref not built")
+def test_port_bit_exact_vs_reference_build_config0(oracle_port, fits002):
+    """Config 0 itself: the 64^3 box (the GPU parity test's input,
+    tissue.box(64, 64, 64)) for 1000 steps, the reference's own code against
+    the port: every Vm, state and activation time identical (so the GPU's
+    config-0 parity against the port is parity against the reference
+    build).  About a minute and a half on 8 cores."""
+    from golden.make_golden import reference_sim
+    from cardioid_b200 import tissue
+    from oracle import refsim
+    refsim.set_threads(os.cpu_count() or 1)
+    t = tissue.box(64, 64, 64)
+    ref = reference_sim(t)
+    ref.set_vm(t.vm0)
+    sim = oracle_port.PortSim(t, fits002, (t.cell_type - 100).astype(np.uint8), 0.02)
+    ref.step(1000)
+    sim.step(1000)
+    np.testing.assert_array_equal(sim.vm(), ref.vm())
+    for k, name in enumerate(ref.field_names()):
+        np.testing.assert_array_equal(sim.state(k), ref.state(name))
+    act = ref.activation()
+    assert (act > 0).sum() > 1000
+    np.testing.assert_array_equal(sim.activation(), act)
+
+
+@pytest.mark.skipif(not _ref_built(), reason="oracle/_ref not built")
 def test_port_masked_tissue_vs_reference_build(oracle_port, fits002):
     """Irregular tissue (a hollow box): FGR boundary weights on an irregular
     mask, bit-exact against the reference."""
