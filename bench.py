@@ -59,6 +59,16 @@ def bench_config(w, world):
                 (ALGO_BYTES["mixed"] - 16) * n / 1e9)}
 
 
+def tuning_overrides(e, stage=None, ctas=None, layout=None):
+    """Profiling runs: forces the staging mode, the CTAs per SM and the tile
+    layout where given (before any tissue is added)."""
+    if layout is not None:
+        e.set_layout(layout)
+    if stage is not None or ctas is not None:
+        st, ct = e.get_tuning()
+        e.set_tuning(st if stage is None else stage, ct if ctas is None else ctas)
+
+
 def read_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -359,11 +369,18 @@ def run_ours(args):
     results = {}
     precs = ("fp64", "mixed") if args.precision == "both" else (args.precision,)
     finals = {}
+    from cardioid_b200 import autotune
     for prec in precs:
+        choice = None
+        if not args.no_autotune and args.stage is None and args.ctas is None and args.layout is None:
+            # tile layout and staging timed on this box (same bits for every choice)
+            choice = autotune.tune(lambda: engine.Engine(DT, precision=prec, device=local),
+                                   lambda e: e.add_tissue(t, engine.transmural_setup(e, t, DT)[0]),
+                                   w["label"].split(":")[0], steps=20, stage_modes=(0, 2, 3), ctas_per_sm=(0,))
         with engine.Engine(DT, precision=prec, device=local) as e:
-            if args.stage is not None or args.ctas is not None:
-                st, ct = e.get_tuning()
-                e.set_tuning(st if args.stage is None else args.stage, ct if args.ctas is None else args.ctas)
+            if choice:
+                autotune.apply(e, choice)
+            tuning_overrides(e, args.stage, args.ctas, args.layout)
             rx, _ = engine.transmural_setup(e, t, DT)
             e.add_tissue(t, rx)
             ms, launches, clocks = time_engine(e, args.steps, args.warmup, world, local)
@@ -374,7 +391,8 @@ def run_ours(args):
             traffic_pc = read_traffic(prec)
             results[prec] = {
                 "value": world * n * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
-                "tuning": {"stage": e.get_tuning()[0], "ctas_per_sm": e.get_tuning()[1]},
+                "tuning": {"layout": e.get_layout(), "stage": e.get_tuning()[0], "ctas_per_sm": e.get_tuning()[1],
+                           "autotune_table_ms_per_step": choice["table"] if choice else None},
                 "gpu_launches": launches, "clocks": clocks,
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_source": peak_src,
@@ -432,8 +450,9 @@ def run_ours(args):
             batch_of(args.steps), args.steps // batch_of(args.steps)),
         "impl": "ours",
         "roofline": m["roofline"],
+        "tuning": m["tuning"],
         "fp64": {"value": f["value"], "ms_per_step": f["ms_per_step"], "roofline": f["roofline"],
-                 "dtype": "f64"},
+                 "dtype": "f64", "tuning": f["tuning"]},
         "mixed_over_fp64": m["value"] / f["value"],
         "mixed_vs_fp64": errors,
         "plain_fp64": plain,
@@ -454,7 +473,7 @@ def _timed_run(e, steps, warmup, world, local):
     return max_over_ranks(ms, world, local), launches, clocks
 
 
-def shell_block(steps, dx, world, rank, local, warmup=3):
+def shell_block(steps, dx, world, rank, local, warmup=3, overrides=None):
     """Irregular anatomy (config 2): the truncated prolate-ellipsoid shell at
     dx mm (20 paced endocardial sites), FP64 and mixed, each timed over
     `steps` steps after `warmup`, and the mixed path's activation-time error
@@ -465,6 +484,7 @@ def shell_block(steps, dx, world, rank, local, warmup=3):
     out, acts = {}, {}
     for prec in ("fp64", "mixed"):
         with engine.Engine(DT, precision=prec, device=local) as e:
+            tuning_overrides(e, **(overrides or {}))
             rid = [e.add_reaction(engine.default_params(c, DT)) for c in (0, 1, 2)]
             tid = e.add_tissue(t, np.array(rid, np.uint8)[rx])
             ms, launches, clocks = _timed_run(e, steps, warmup, world, local)
@@ -483,11 +503,15 @@ def shell_block(steps, dx, world, rank, local, warmup=3):
                               "activation_max_err_ms": float(np.abs(a[both] - b[both]).max()) if both.any() else None}}
 
 
+def overrides_of(args):
+    return {"stage": args.stage, "ctas": args.ctas, "layout": args.layout}
+
+
 def run_shell(args):
     world, rank, local = dist_setup()
     import torch
     torch.cuda.set_device(local)
-    line = shell_block(args.steps, args.shell_dx, world, rank, local)
+    line = shell_block(args.steps, args.shell_dx, world, rank, local, overrides=overrides_of(args))
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -544,7 +568,7 @@ def run_batch(args):
                           % (len(insts), pop.total_cells(insts), args.steps, DT), **out}), flush=True)
 
 
-def serve_block(n_jobs, rate, job_steps, job_beats, precisions, serve_batch, world, rank, local):
+def serve_block(n_jobs, rate, job_steps, job_beats, precisions, serve_batch, world, rank, local, overrides=None):
     """Serving (config 4): Poisson job arrivals with config 4's size and
     parameter distributions, continuous batching in one engine per
     precision; p50/p99 time-to-result and aggregate cell-steps/s.  Each job
@@ -556,6 +580,7 @@ def serve_block(n_jobs, rate, job_steps, job_beats, precisions, serve_batch, wor
     out = {}
     for prec in precisions:
         with engine.Engine(DT, precision=prec, device=local) as e:
+            tuning_overrides(e, **(overrides or {}))
             rid = [e.add_reaction(engine.default_params(c, DT)) for c in (0, 1, 2)]
             srv = serving.Server(e, rid, batch=serve_batch)
             res = srv.run(jobs)
@@ -573,7 +598,7 @@ def run_serve(args):
     import torch
     torch.cuda.set_device(local)
     line = serve_block(args.jobs, args.rate, args.job_steps, args.job_beats, ("mixed", "fp64"), args.serve_batch,
-                       world, rank, local)
+                       world, rank, local, overrides=overrides_of(args))
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -689,7 +714,8 @@ def main():
     ap.add_argument("--shell-dx", type=float, default=0.25)
     ap.add_argument("--instances", type=int, default=4096)
     ap.add_argument("--batch-precisions", default="mixed,fp64")
-    ap.add_argument("--no-autotune", action="store_true", help="config 3: keep the default tile layout and launch")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the engine's default tile layout and launch (no timing of the candidates first)")
     ap.add_argument("--jobs", type=int, default=200, help="jobs of --config serve")
     ap.add_argument("--line-jobs", type=int, default=24, help="jobs of the serving block in the headline line")
     ap.add_argument("--rate", type=float, default=5.0, help="job arrivals per second (serving)")
@@ -713,6 +739,7 @@ def main():
     ap.add_argument("--stage", type=int, choices=[0, 1, 2, 3], default=None,
                     help="profiling runs: the step kernel's staging mode (default: the engine's)")
     ap.add_argument("--ctas", type=int, default=None, help="profiling runs: CTAs per SM of the persistent grid")
+    ap.add_argument("--layout", choices=["cells", "rows"], default=None, help="profiling runs: warp-tile layout")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

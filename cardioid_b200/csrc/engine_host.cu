@@ -202,14 +202,15 @@ struct Engine {
   int graphSteps = 0;
   bool graphMinmax = false;
   // launch tuning (cdb_engine_set_tuning; the autotuner picks them)
-  int stage = 1;           // 1: stage each warp's next tile through shared memory (cp.async)
+  int stage = 0;           // staging mode (set per precision at creation)
   bool withhold = false;   // cdb_engine_test_bounded_wait: the next batch withholds its bulk copies
   int ctasPerSm = 0;       // persistent grid: SMs x this; 0 = as many as are resident
-  int layout = CDB_LAYOUT_CELLS;   // warp-tile layout of tissues added from here on
+  int layout = CDB_LAYOUT_ROWS;    // warp-tile layout of tissues added from here on
   int numSms = 148;
   // resident CTAs per SM by [stage][ECG][slot] (last: generic)
   int resident[4][2][CDB_MAX_REACTION_TYPES + 1] = {};
   bool anyEcg = false;     // a tissue has ECG electrodes: launch the kernels with the sensor
+  bool windowSlot[CDB_MAX_REACTION_TYPES] = {};   // stage 3 runs this type's launches with Vm windows
 
   int grid_ctas_per_sm(int slot, int st)
   {
@@ -325,6 +326,12 @@ struct Engine {
     }
     slotTiles.clear();
     for (int sl = 0; sl < CDB_MAX_REACTION_TYPES; ++sl) {
+      // stage 3 uses the window variant for a type's launches only when at
+      // least half of its tiles are row tiles (the variant runs the others
+      // slower than stage 2: stencil after the reaction, weights unstaged)
+      int64_t rows = 0;
+      for (const WarpTile& tl : bySlot[sl]) rows += (tl.flags & kTileRow) ? 1 : 0;
+      windowSlot[sl] = !bySlot[sl].empty() && 2 * rows >= (int64_t)bySlot[sl].size();
       if (bySlot[sl].empty()) continue;
       slotTiles.push_back({sl, {(int)tiles.size(), (int)bySlot[sl].size()}});
       tiles.insert(tiles.end(), bySlot[sl].begin(), bySlot[sl].end());
@@ -378,7 +385,7 @@ struct Engine {
     a.dt = cfg.dt;
     a.k = s;
     a.minmax = minmax ? 1 : 0;
-    a.stage = withhold ? 2 : stage;
+    a.stage = withhold ? 2 : (stage == 3 && !windowSlot[rt]) ? 2 : stage;
     a.err = dErr.as<int>();
     a.withhold = withhold ? 1 : 0;
     a.nTissues = (int)order.size();
@@ -835,7 +842,7 @@ int64_t tissue_bytes(const Engine& E, const cdb_tissue_desc* t)
   int64_t count[CDB_MAX_REACTION_TYPES];
   const int64_t nSlots = count_slots(n, t->reaction, E.slots, count);
   const bool mixed = E.cfg.precision == CDB_MIXED;
-  int64_t b = 2 * (vox + kVmTail) * 8;                                       // Vm blocks
+  int64_t b = 2 * vox * 8;                                                   // Vm blocks
   b += mixed ? nSlots * (kRowsMixed64 * 8 + kRowsMixed32 * 4) : nSlots * kRows64 * 8;   // state
   b += nSlots * weight_rows(cls, mixed) * (mixed ? 4 : 8);                   // weights
   b += nSlots * (8 + 4) + n * 8 + (masked ? n * 8 : 0) + 64;                 // act, vrel, slot map, voxel
@@ -896,7 +903,9 @@ cdb_status cdb_engine_create(const cdb_engine_config* cfg, cdb_engine** out)
   CDB_CUDA(cudaMemset(e->e.dErr.p, 0, sizeof(int)));
   // measured on the 256^3 box: bulk-copy staging is fastest for the mixed
   // step (1.02 ms against 1.10 with cp.async); FP64 keeps direct loads
-  e->e.stage = cfg->precision == CDB_MIXED ? 2 : 0;
+  // defaults: the autotuner's choice on the 256^3 box (mixed: row tiles with
+  // their Vm window by TMA; FP64: direct loads)
+  e->e.stage = cfg->precision == CDB_MIXED ? 3 : 0;
   CDB_CUDA(cfg->precision == CDB_MIXED ? allow_step_smem<true>() : allow_step_smem<false>());
   *out = e.release();
   return CDB_OK;
@@ -1025,11 +1034,10 @@ cdb_status cdb_engine_add_tissue(cdb_engine* e, const cdb_tissue_desc* t, int32_
 
   cudaStream_t s = E.stream;
   CDB_CUDA(cudaStreamSynchronize(s));
-  // (+ kVmTail zeroed doubles, read by stage 3's window rows at the block's end)
-  CDB_CUDA(h->vm0.alloc((vox + kVmTail) * 8));
-  CDB_CUDA(h->vm1.alloc((vox + kVmTail) * 8));
-  CDB_CUDA(cudaMemsetAsync(h->vm0.p, 0, (vox + kVmTail) * 8, s));
-  CDB_CUDA(cudaMemsetAsync(h->vm1.p, 0, (vox + kVmTail) * 8, s));
+  CDB_CUDA(h->vm0.alloc(vox * 8));
+  CDB_CUDA(h->vm1.alloc(vox * 8));
+  CDB_CUDA(cudaMemsetAsync(h->vm0.p, 0, vox * 8, s));
+  CDB_CUDA(cudaMemsetAsync(h->vm1.p, 0, vox * 8, s));
   // slots grouped by reaction type; AoSoA arrays cover whole 32-slot blocks
   std::vector<int32_t> vrel;
   {

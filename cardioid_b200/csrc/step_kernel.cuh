@@ -198,8 +198,6 @@ constexpr int kWinBytes = 9 * kWinRow * 8;
 // dynamic shared memory and each warp's window takes a multiple of 128.
 __host__ __device__ constexpr int align128(int b) { return (b + 127) / 128 * 128; }
 constexpr int kWinStride = align128(kWinBytes);
-// Padded Vm blocks carry this many zeroed doubles past their last voxel.
-constexpr int64_t kVmTail = 64;
 
 // Dynamic shared memory of a launch: per warp two staging buffers (stages
 // 1-3), three mbarriers (stages 2-3: the two buffers and the window) and,
@@ -751,8 +749,11 @@ __device__ __forceinline__ bool step_tile(const StepArgs& a, const WarpTile& til
 #ifndef CDB_FP64_MIN_CTAS
 #define CDB_FP64_MIN_CTAS 4
 #endif
+#ifndef CDB_MIXED_MIN_CTAS
+#define CDB_MIXED_MIN_CTAS 5
+#endif
 template <bool MIXED>
-constexpr int min_ctas() { return MIXED ? 5 : CDB_FP64_MIN_CTAS; }
+constexpr int min_ctas() { return MIXED ? CDB_MIXED_MIN_CTAS : CDB_FP64_MIN_CTAS; }
 
 // Persistent over the launch's warp tiles: warp w takes tiles w, w + W,
 // w + 2W, ... (W warps in the grid).  With a.stage set, the next tile's

@@ -227,16 +227,16 @@ class Engine:
         memory, 2 = bulk (TMA) copies into shared memory completing on an
         mbarrier, 3 = as 2, plus the Vm tile and halo of each row tile (the
         nine stencil rows of 32 consecutive voxels of a volume tissue) copied
-        into shared memory while the reaction computes (defaults: 2 mixed,
+        into shared memory while the reaction computes (defaults: 3 mixed,
         0 FP64; every stage gives the same bits); ctas_per_sm sizes the
         persistent grid (0: as many CTAs per SM as are resident)."""
         _lib.check(_lib.load().cdb_engine_set_tuning(self.h, int(stage), int(ctas_per_sm)))
 
     def set_layout(self, layout):
         """Warp-tile layout of tissues added from now on: "cells" (each
-        reaction type's cells in cell order, 32 per tile) or "rows" (every
-        x-row run of a type cut into whole 32-cell row tiles, remainders
-        packed).  Same results bit for bit."""
+        reaction type's cells in cell order, 32 per tile) or "rows" (the
+        default: every x-row run of a type cut into whole 32-cell row tiles,
+        remainders packed).  Same results bit for bit."""
         code = {"cells": 0, "rows": 1}[layout]
         _lib.check(_lib.load().cdb_engine_set_layout(self.h, code))
 

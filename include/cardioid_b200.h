@@ -306,18 +306,20 @@ cdb_status cdb_diag_fit_forms(const cdb_fit fits[CDB_NUM_FITS], int32_t poolSize
  * the same with bulk (TMA) copies completing on an mbarrier, 3 = stage 2
  * plus the Vm tile and halo of every row tile (32 consecutive voxels of one
  * x-row of a volume tissue with even padded strides): its nine stencil rows
- * are bulk-copied into shared memory while the reaction computes and the
- * stencil reads them there, 0 = direct loads; ctasPerSm sizes the
+ * are loaded into shared memory by one TMA tensor copy while the reaction
+ * computes and the stencil reads them there (a reaction type's launches run
+ * as stage 2 when fewer than half of its tiles are row tiles), 0 = direct
+ * loads; ctasPerSm sizes the
  * persistent grid (SMs x ctasPerSm CTAs of 128 threads), 0 = as many CTAs as
  * are resident on an SM at once.  All stages give the same results bit for
- * bit.  Defaults: stage 2 for CDB_MIXED, 0 for CDB_FP64, ctasPerSm 0;
+ * bit.  Defaults: stage 3 for CDB_MIXED, 0 for CDB_FP64, ctasPerSm 0;
  * cardioid_b200.autotune picks them by timing. */
 cdb_status cdb_engine_set_tuning(cdb_engine* e, int32_t stage, int32_t ctasPerSm);
 cdb_status cdb_engine_get_tuning(cdb_engine* e, int32_t* stage, int32_t* ctasPerSm);
 
 /* Warp-tile layout of the tissues added after the call (no counterpart in
- * the reference): CDB_LAYOUT_CELLS (default) fills each reaction type's
- * 32-slot blocks with its cells in cell order; CDB_LAYOUT_ROWS cuts every
+ * the reference): CDB_LAYOUT_CELLS fills each reaction type's 32-slot
+ * blocks with its cells in cell order; CDB_LAYOUT_ROWS (default) cuts every
  * x-row run of a type into whole 32-cell row tiles (stage 3 stages their
  * Vm tile and halo) and packs the runs' remainders into shared blocks.  Same
  * results bit for bit; cardioid_b200.autotune picks it by timing. */

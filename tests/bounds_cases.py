@@ -27,7 +27,8 @@ def masked(nx, ny, nz, seed=3):
 
 def rows(nx, ny, nz):
     """One cell type, x-rows of whole warp tiles: stage 3's Vm windows, the
-    last one reading past the padded block's last voxel."""
+    last one's TMA box reaching past the padded block's x extent (read as
+    zeros)."""
     t = tissue.box(nx, ny, nz)
     t.cell_type[:] = 100
     return t
