@@ -423,7 +423,8 @@ def run_ours(args):
     if args.precision != "both" or args.no_e2e:
         # a profiling run: one line per precision, no headline
         for prec in precs:
-            print(json.dumps({"config": w["label"], "precision": prec, "steps": args.steps, **results[prec]}),
+            extra = {"e2e": results["e2e"]} if prec == "mixed" and "e2e" in results else {}
+            print(json.dumps({"config": w["label"], "precision": prec, "steps": args.steps, **results[prec], **extra}),
                   flush=True)
         return
     m, f = results["mixed"], results["fp64"]

@@ -1,9 +1,9 @@
 """cdb_fgr_calc_static, the FGR stencil for callers that cannot allocate
 device memory (it keeps its padded Vm block in a static device array),
 against the allocating entry points cdb_fgr_create / _update_local_voltage /
-_calc, for two calls in a row: first on a larger box, then on a smaller one,
-so the first call's values sit where the second call's halo is (the second
-call must clear them).  A warmed-up call leaves the device's free memory
+_calc and against the oracle's stencil, for two calls in a row: first on a
+larger box, then on a smaller one, so the first call's values sit where the
+second call's halo is (the second call must clear them).  A warmed-up call leaves the device's free memory
 unchanged and the calling thread's current device as it was.
 
 This file is collected last so that a run stopping at the first failure has
@@ -40,7 +40,17 @@ def _case(t, scale, seed):
     return w19, vm, want.cpu().numpy()
 
 
-def test_static_scratch_stencil_matches_allocating_path_twice(cdb_lib):
+def _oracle_dvmd(oracle_port, fits, t, vm):
+    """The oracle's diffusion term for voltage vm (the FGR stencil of one
+    step taken from vm, elec/FGRDiffusionOMP.cc:109-131)."""
+    sim = oracle_port.PortSim(t, fits, (t.cell_type - 100).astype(np.uint8), 0.02)
+    sim.set_vm(vm)
+    sim.step(1)
+    return sim.dvm()[1]
+
+
+def test_static_scratch_stencil_matches_allocating_path_twice(cdb_lib, oracle_port, fits002):
+    """Each call against the allocating plugin and against the oracle."""
     import torch
     stream = torch.cuda.current_stream().cuda_stream
     for call, t in enumerate((tissue.box(23, 17, 11, seed=9), tissue.box(11, 9, 7, seed=10))):
@@ -51,6 +61,8 @@ def test_static_scratch_stencil_matches_allocating_path_twice(cdb_lib):
         g = got.cpu().numpy()
         assert np.isfinite(g).all()
         assert np.abs(g - want).max() <= REL_TOL * np.abs(want).max(), call
+        ref = _oracle_dvmd(oracle_port, fits002, t, vm.cpu().numpy())
+        assert np.abs(g - ref).max() <= REL_TOL * np.abs(ref).max(), call
 
 
 def test_static_scratch_allocates_nothing(cdb_lib):
