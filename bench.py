@@ -435,6 +435,7 @@ def run_ours(args):
               "activation_max_err_ms": float(np.abs(af[both] - am[both]).max()) if both.any() else None,
               "full_beat": apd_check(local) if world == 1 and not args.no_apd else None}
     plain = time_plain_fp64(t, args, local) if world == 1 and not args.no_plain else None
+    ref_gpu = reference_gpu_block(t, local) if world == 1 and not args.no_plain else None
     # configs 2 and 4 in the same line (one GPU only, to keep the run short)
     shell_line = shell_block(args.shell_steps, args.shell_dx, world, rank, local) \
         if world == 1 and not args.no_shell else None
@@ -458,6 +459,7 @@ def run_ours(args):
         "mixed_vs_fp64": errors,
         "plain_fp64": plain,
         "mixed_over_plain_fp64": (m["value"] / plain["value"]) if plain else None,
+        "reference_gpu_reaction": ref_gpu,
         "e2e": results["e2e"],
         "shell": shell_line,
         "serve": serve_line,
@@ -679,6 +681,48 @@ def time_plain_fp64(t, args, local):
     return {"value": t.n * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps, "dtype": "f64",
             "path": "split loop on the plugins: 3 x cdb_reaction_calc + cdb_fgr_update_local_voltage + cdb_fgr_calc "
                     "+ stimulus and Vm update as tensor ops (CUDA events, default stream)"}
+
+
+def reference_gpu_block(t, local, steps=20, warmup=3):
+    """The reference's own GPU reaction (BetterTT06's NVRTC kernel through its
+    ReactionManager::calc, oracle/_ref/ref_gpu_reaction, in a child process)
+    beside the plugin reaction (plugins.ReactionManager over
+    cdb_reaction_calc) on the box's cells: FP64, Vm and iStim fixed at the
+    resting state, `steps` calls after `warmup`, CUDA events on each side's
+    launching stream.  The reference's GPU diffusion (CUDADiffusion) is not
+    run: its kernel returns from threads before a __syncthreads."""
+    from oracle import refgpu
+    if not refgpu.available():
+        return None
+    import torch
+    from cardioid_b200 import engine, objectdb, plugins, tissue
+    info, _, _ = refgpu.run(t.cell_type, DT, steps, warmup)
+    db = objectdb.ObjectDB()
+    for ct in (0, 1, 2):
+        db.compile_file(engine.shipped_fit_path(DT, ct))
+    db.compile(tissue.reaction_objects_text(["tt06Endo_fit", "tt06Mid_fit", "tt06Epi_fit"]))
+    rm = plugins.ReactionManager(db, list(refgpu.NAMES), DT, t.cell_type, device=local)
+    Vm = torch.zeros(t.n, dtype=torch.float64, device="cuda:%d" % local)
+    rm.initializeMembraneState(Vm)
+    iStim, dVm = torch.zeros_like(Vm), torch.zeros_like(Vm)
+    for _ in range(warmup):
+        rm.calc(DT, Vm, iStim, dVm)
+    torch.cuda.synchronize(local)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(steps):
+        rm.calc(DT, Vm, iStim, dVm)
+    s1.record()
+    s1.synchronize()
+    ms = s0.elapsed_time(s1) / steps
+    del rm
+    ours = {"value": t.n / (ms / 1e3), "ms_per_step": ms}
+    ref = {"value": info["cell_steps_per_s"], "ms_per_step": info["ms_per_step"]}
+    return {"reference": ref, "ours_plugin": ours, "ours_over_reference": ours["value"] / ref["value"],
+            "unit": METRIC, "steps": steps, "warmup": warmup, "dtype": "f64",
+            "what": "reaction only (3 BetterTT06 types, Vm and iStim fixed): the reference's NVRTC kernel "
+                    "through its ReactionManager::calc, built from its sources with USE_CUDA, against "
+                    "plugins.ReactionManager over cdb_reaction_calc; the reference's GPU diffusion is not run"}
 
 
 def run_reference(args):

@@ -1,0 +1,75 @@
+"""Runs the reference's own GPU reaction path (oracle/_ref/ref_gpu_reaction:
+BetterTT06 compiled with USE_CUDA, its NVRTC kernel driven through the
+reference's ReactionManager::calc, elec/BetterTT06.cc:1004-1410 and
+elec/ReactionManager.cc:14-27) on a set of cells, in a child process.
+
+TEST AND MEASUREMENT INFRASTRUCTURE.  Only tests/ and bench.py use it, as
+a checker and as the reference's GPU comparison point; the product never
+imports it.
+"""
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BINARY = os.path.join(HERE, "_ref", "ref_gpu_reaction")
+NAMES = ("tt06Endo", "tt06Mid", "tt06Epi")
+
+
+def available():
+    return os.path.exists(BINARY)
+
+
+def objects_text(dt):
+    """The three transmural BetterTT06 REACTION objects on the shipped fits
+    (anatomy cellType 100/101/102 -> celltype 0/1/2)."""
+    from cardioid_b200 import engine, tissue
+    text = ""
+    for ct in (0, 1, 2):
+        with open(engine.shipped_fit_path(dt, ct)) as f:
+            text += f.read()
+    return text + tissue.reaction_objects_text(["tt06Endo_fit", "tt06Mid_fit", "tt06Epi_fit"])
+
+
+def run(cell_type, dt, steps, warmup=0, vm=None, outputs=False, timeout=600):
+    """Steps the reference's GPU reaction `warmup` + `steps` times with Vm
+    and iStim fixed (cells in the given order, anatomy cellTypes 100-102).
+
+    Returns (info, dvm, states): info is the driver's JSON line (cells,
+    ms_per_step over the `steps` timed calls, cell_steps_per_s); with
+    `outputs`, dvm (float64[n]) and the checkpoint states after the last
+    call ({name: float64[n]}, the reference's getCheckpointInfo order).
+    """
+    if not available():
+        raise RuntimeError("oracle/_ref/ref_gpu_reaction is not built (make -C oracle/ref gpu)")
+    ct = np.ascontiguousarray(cell_type, dtype=np.int32)
+    n = ct.size
+    with tempfile.TemporaryDirectory() as tmp:
+        obj = os.path.join(tmp, "objects.data")
+        with open(obj, "w") as f:
+            f.write(objects_text(dt))
+        ct_path = os.path.join(tmp, "celltype.bin")
+        ct.tofile(ct_path)
+        vm_path = "-"
+        if vm is not None:
+            vm_path = os.path.join(tmp, "vm.bin")
+            np.ascontiguousarray(vm, dtype=np.float64).tofile(vm_path)
+        out_path = os.path.join(tmp, "out.bin") if outputs else "-"
+        cmd = [BINARY, obj, repr(dt), str(steps), str(warmup), ct_path, vm_path, out_path] + list(NAMES)
+        # cwd: a fit the reference had to generate would be written there
+        res = subprocess.run(cmd, cwd=tmp, capture_output=True, text=True, timeout=timeout)
+        if res.returncode != 0:
+            raise RuntimeError("ref_gpu_reaction failed (%d): %s" % (res.returncode, res.stderr[-2000:]))
+        info = json.loads(res.stdout.strip().splitlines()[-1])
+        if not outputs:
+            return info, None, None
+        raw = np.fromfile(out_path, dtype=np.float64)
+    from cardioid_b200 import tt06
+    names = list(tt06.STATE_NAMES)
+    if raw.size != n * (1 + len(names)):
+        raise RuntimeError("ref_gpu_reaction wrote %d values, expected %d" % (raw.size, n * (1 + len(names))))
+    cols = raw.reshape(1 + len(names), n)
+    return info, cols[0].copy(), {nm: cols[1 + k].copy() for k, nm in enumerate(names)}
