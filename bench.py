@@ -600,8 +600,8 @@ def run_serve(args):
     world, rank, local = dist_setup()
     import torch
     torch.cuda.set_device(local)
-    line = serve_block(args.jobs, args.rate, args.job_steps, args.job_beats, ("mixed", "fp64"), args.serve_batch,
-                       world, rank, local, overrides=overrides_of(args))
+    line = serve_block(args.jobs, args.rate, args.job_steps, args.job_beats, tuple(args.serve_precisions.split(",")),
+                       args.serve_batch, world, rank, local, overrides=overrides_of(args))
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -771,6 +771,7 @@ def main():
     ap.add_argument("--no-shell", action="store_true", help="skip the shell (config 2) block of the headline line")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving (config 4) block of the headline line")
     ap.add_argument("--serve-batch", type=int, default=250)
+    ap.add_argument("--serve-precisions", default="mixed,fp64", help="precisions of --config serve")
     ap.add_argument("--e2e-steps", type=int, default=50)
     ap.add_argument("--cpu-steps", type=int, default=20, help="steps per CPU slab process (cpu_baseline)")
     ap.add_argument("--cpu-omp-steps", type=int, default=2,
