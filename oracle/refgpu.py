@@ -1,7 +1,8 @@
-"""Runs the reference's own GPU reaction path (oracle/_ref/ref_gpu_reaction:
-BetterTT06 compiled with USE_CUDA, its NVRTC kernel driven through the
-reference's ReactionManager::calc, elec/BetterTT06.cc:1004-1410 and
-elec/ReactionManager.cc:14-27) on a set of cells, in a child process.
+"""Runs the reference's own GPU code in child processes: its reaction path
+(oracle/_ref/ref_gpu_reaction: BetterTT06 compiled with USE_CUDA, its NVRTC
+kernel driven through the reference's ReactionManager::calc,
+elec/BetterTT06.cc:1004-1410 and elec/ReactionManager.cc:14-27) and its ECG
+kernels (oracle/_ref/ref_gpu_ecg: elec/ECGSensor.cu).
 
 TEST AND MEASUREMENT INFRASTRUCTURE.  Only tests/ and bench.py use it, as
 a checker and as the reference's GPU comparison point; the product never
@@ -73,3 +74,37 @@ def run(cell_type, dt, steps, warmup=0, vm=None, outputs=False, timeout=600):
         raise RuntimeError("ref_gpu_reaction wrote %d values, expected %d" % (raw.size, n * (1 + len(names))))
     cols = raw.reshape(1 + len(names), n)
     return info, cols[0].copy(), {nm: cols[1 + k].copy() for k, nm in enumerate(names)}
+
+
+ECG_BINARY = os.path.join(HERE, "_ref", "ref_gpu_ecg")
+
+
+def ecg_available():
+    return os.path.exists(ECG_BINARY)
+
+
+def ecg(t, points, dvmd=None, timeout=300):
+    """The reference's own ECG kernels on the GPU (oracle/_ref/ref_gpu_ecg:
+    calcInvrCUDA and calcEcgCUDA of elec/ECGSensor.cu) for tissue t's cells
+    and the electrodes `points` ([m, 3], mm): returns (invr [n, m], sums [m]
+    or None), sums[j] = sum over cells of dvmd[i] invr[i, j] when dvmd is
+    given (no kconst or voxel-volume factor: ECGSensor applies those)."""
+    if not ecg_available():
+        raise RuntimeError("oracle/_ref/ref_gpu_ecg is not built (make -C oracle/ref gpu)")
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+    n, m = len(t.gid), len(pts)
+    with tempfile.TemporaryDirectory() as tmp:
+        gp, pp, op = (os.path.join(tmp, f) for f in ("gid.bin", "points.bin", "out.bin"))
+        np.ascontiguousarray(t.gid, dtype=np.int64).tofile(gp)
+        pts.tofile(pp)
+        dp = "-"
+        if dvmd is not None:
+            dp = os.path.join(tmp, "dvmd.bin")
+            np.ascontiguousarray(dvmd, dtype=np.float64).tofile(dp)
+        cmd = [ECG_BINARY, str(t.nx), str(t.ny), str(t.nz), repr(t.dx), repr(t.dy), repr(t.dz), gp, pp, dp, op]
+        res = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+        if res.returncode != 0:
+            raise RuntimeError("ref_gpu_ecg failed (%d): %s" % (res.returncode, res.stderr[-2000:]))
+        raw = np.fromfile(op, dtype=np.float64)
+    invr = raw[:n * m].reshape(n, m)
+    return invr, (raw[n * m:n * m + m].copy() if dvmd is not None else None)

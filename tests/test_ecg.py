@@ -109,3 +109,43 @@ def test_ecg_ring_keeps_the_latest_evaluations(cdb_lib, fits002):
         e.set_ecg(tid, POINTS[:0], 1, 1.0)   # off
         e.step(2)
         assert len(e.read_ecg(tid)[0]) == 0
+
+
+@pytest.mark.gpu
+def test_reference_gpu_ecg_kernels(cdb_lib, oracle_port, fits002):
+    """The reference's own ECG kernels (calcInvrCUDA, calcEcgCUDA of
+    elec/ECGSensor.cu, built from its source by oracle/ref/Makefile and run
+    on the GPU) against the restatement above and the fused sensor:
+    - the 1/r table equals the restatement's to 1e-15 relative (the kernel
+      contracts the squared distance into FMAs; IEEE sqrt and division);
+    - its sum over the oracle's dVmD equals the restatement's within 1e-13
+      of the sum of |terms| (atomic, blocked summation order);
+    - the fused sensor's FP64 trace at the same step equals kconst dx dy dz
+      times that sum, within 1e-9 of its size (the FP64 tolerance above).
+    The box's 2688 cells are a multiple of 112, where the reference's sum
+    kernel stays inside the cell array."""
+    from cardioid_b200 import engine as eng_mod
+    from oracle import refgpu
+    if not refgpu.ecg_available():
+        pytest.skip("oracle/_ref/ref_gpu_ecg not built (needs the reference checkout at build time)")
+    t = tissue.box(16, 14, 12, period=6.0)
+    assert t.n % 112 == 0
+    rx = (t.cell_type - 100).astype(np.uint8)
+    sim = oracle_port.PortSim(t, fits002, rx, 0.02)
+    steps = 40
+    sim.step(steps)
+    dvmd = sim.dvm()[1]
+    invr, sums = refgpu.ecg(t, POINTS, dvmd)
+    np.testing.assert_allclose(invr, invr_table(t, POINTS), rtol=1e-15, atol=0)
+    bound = 1e-13 * (np.abs(invr) * np.abs(dvmd)[:, None]).sum(axis=0)
+    assert (np.abs(sums - ecg_sum(invr, dvmd)) <= bound).all()
+    want = KCONST * t.dx * t.dy * t.dz * sums
+    with eng_mod.Engine(0.02, precision="fp64") as e:
+        for p in fits002:
+            e.add_reaction(p)
+        tid = e.add_tissue(t, rx)
+        e.set_ecg(tid, POINTS, steps, KCONST)
+        e.step(steps)
+        loops, got = e.read_ecg(tid)
+    np.testing.assert_array_equal(loops, [steps])
+    assert np.abs(got[0] - want).max() <= 1e-9 * np.abs(want).max()
