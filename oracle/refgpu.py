@@ -2,7 +2,8 @@
 (oracle/_ref/ref_gpu_reaction: BetterTT06 compiled with USE_CUDA, its NVRTC
 kernel driven through the reference's ReactionManager::calc,
 elec/BetterTT06.cc:1004-1410 and elec/ReactionManager.cc:14-27) and its ECG
-kernels (oracle/_ref/ref_gpu_ecg: elec/ECGSensor.cu).
+kernels (oracle/_ref/ref_gpu_ecg: elec/ECGSensor.cu) and "cuda" Diffusion
+(oracle/_ref/ref_gpu_diff6: elec/CUDADiffusion.cc with its kernels).
 
 TEST AND MEASUREMENT INFRASTRUCTURE.  Only tests/ and bench.py use it, as
 a checker and as the reference's GPU comparison point; the product never
@@ -108,3 +109,36 @@ def ecg(t, points, dvmd=None, timeout=300):
         raw = np.fromfile(op, dtype=np.float64)
     invr = raw[:n * m].reshape(n, m)
     return invr, (raw[n * m:n * m + m].copy() if dvmd is not None else None)
+
+
+DIFF6_BINARY = os.path.join(HERE, "_ref", "ref_gpu_diff6")
+
+
+def diff6_available():
+    return os.path.exists(DIFF6_BINARY)
+
+
+def diff6(t, vm, scale, timeout=300):
+    """dVm from the reference's own "cuda" Diffusion on the GPU
+    (oracle/_ref/ref_gpu_diff6: CUDADiffusion with diff_6face_v1, one
+    updateLocalVoltage + calc as the omp loop calls them) for tissue t and
+    Vm `vm`, diffusion scale `scale`.  t's extents in y and z must be
+    multiples of 30 (the driver refuses other shapes: there the reference
+    kernel returns from threads before its barriers)."""
+    if not diff6_available():
+        raise RuntimeError("oracle/_ref/ref_gpu_diff6 is not built (make -C oracle/ref gpu)")
+    n = len(t.gid)
+    with tempfile.TemporaryDirectory() as tmp:
+        paths = [os.path.join(tmp, f) for f in ("gid.bin", "ct.bin", "sigma.bin", "vm.bin", "out.bin")]
+        np.ascontiguousarray(t.gid, dtype=np.int64).tofile(paths[0])
+        np.ascontiguousarray(t.cell_type, dtype=np.int32).tofile(paths[1])
+        np.ascontiguousarray(t.sigma, dtype=np.float64).reshape(-1).tofile(paths[2])
+        np.ascontiguousarray(vm, dtype=np.float64).tofile(paths[3])
+        cmd = [DIFF6_BINARY, str(t.nx), str(t.ny), str(t.nz), repr(t.dx), repr(t.dy), repr(t.dz), repr(scale)] + paths
+        res = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+        if res.returncode != 0:
+            raise RuntimeError("ref_gpu_diff6 failed (%d): %s" % (res.returncode, res.stderr[-2000:]))
+        out = np.fromfile(paths[4], dtype=np.float64)
+    if out.size != n:
+        raise RuntimeError("ref_gpu_diff6 wrote %d values, expected %d" % (out.size, n))
+    return out

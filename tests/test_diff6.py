@@ -7,8 +7,10 @@ The face-conductivity table is pinned to the reference's own code: the
 oracle build constructs the reference's CUDADiffusion (its constructor
 builds the table on the host, elec/CUDADiffusion.cc:73-122), and both the
 restatement (CPU) and the plugin (GPU) reproduce it bit for bit.  The
-reference's kernel (diff_6face_v1) is not run: it returns from threads
-before a __syncthreads."""
+reference's kernel (diff_6face_v1) returns from threads before a
+__syncthreads unless the local grid's y and z sizes are 30 k + 2; on such
+tissues the reference's own "cuda" Diffusion runs on the GPU
+(oracle/_ref/ref_gpu_diff6) and the plugin's dVm is checked against it."""
 import numpy as np
 import pytest
 
@@ -87,3 +89,47 @@ def test_diff6_plugin_matches_oracle(cdb_lib, kind):
     ref = diff6.calc(t, vm, 714.2857)
     got = out.cpu().numpy()
     assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+def _tissues30():
+    """Tissues whose y and z extents are 30 (local grid 30 k + 2), the only
+    shapes the reference kernel runs on without returning from threads
+    before its barriers: a rotated-fibre box and the same box with a hole
+    and a notch (extents kept)."""
+    box = tissue.box(23, 30, 30, seed=4)
+    x, y, z = box.tuples()
+    keep = ~((x >= 8) & (x <= 14) & (y >= 10) & (y <= 17) & (z >= 5) & (z <= 20))
+    keep &= ~((x == 22) & (y < 6))
+    masked = tissue.Tissue(box.nx, box.ny, box.nz, box.dx, box.dy, box.dz, box.gid[keep], box.cell_type[keep],
+                           box.sigma[keep], box.vm0[keep], [])
+    return {"box": box, "masked": masked}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["box", "masked"])
+def test_diff6_plugin_matches_reference_kernel(cdb_lib, oracle_port, kind):
+    """The plugin against the reference's own "cuda" Diffusion run on the
+    GPU (CUDADiffusion.cc and diff_6face_v1 built from the reference
+    sources, oracle/_ref/ref_gpu_diff6): dVm within 1e-12 of the largest
+    |dVm| (the two sum the face fluxes in different orders), and the numpy
+    restatement within the same bound."""
+    import torch
+    from cardioid_b200 import plugins
+    from oracle import diff6, refgpu
+    if not refgpu.diff6_available():
+        pytest.skip("oracle/_ref/ref_gpu_diff6 not built (needs the reference checkout at build time)")
+    t = _tissues30()[kind]
+    rng = np.random.default_rng(11)
+    vm = -80.0 + 40.0 * rng.random(t.n)
+    ref = refgpu.diff6(t, vm, t.diffusion_scale)
+    scale = np.abs(ref).max()
+    assert scale > 0
+    d = plugins.CUDADiffusion(t, t.diffusion_scale)
+    V = torch.tensor(vm, device="cuda")
+    out = torch.empty_like(V)
+    d.updateLocalVoltage(V)
+    d.calc(out)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    assert np.abs(got - ref).max() <= 1e-12 * scale, np.abs(got - ref).max() / scale
+    assert np.abs(diff6.calc(t, vm, t.diffusion_scale) - ref).max() <= 1e-12 * scale
