@@ -436,6 +436,7 @@ def run_ours(args):
               "full_beat": apd_check(local) if world == 1 and not args.no_apd else None}
     plain = time_plain_fp64(t, args, local) if world == 1 and not args.no_plain else None
     ref_gpu = reference_gpu_block(t, local) if world == 1 and not args.no_plain else None
+    ref_gpu_diff = reference_gpu_diffusion_block(local) if world == 1 and not args.no_plain else None
     # configs 2 and 4 in the same line (one GPU only, to keep the run short)
     shell_line = shell_block(args.shell_steps, args.shell_dx, world, rank, local) \
         if world == 1 and not args.no_shell else None
@@ -460,6 +461,7 @@ def run_ours(args):
         "plain_fp64": plain,
         "mixed_over_plain_fp64": (m["value"] / plain["value"]) if plain else None,
         "reference_gpu_reaction": ref_gpu,
+        "reference_gpu_diffusion": ref_gpu_diff,
         "e2e": results["e2e"],
         "shell": shell_line,
         "serve": serve_line,
@@ -689,8 +691,10 @@ def reference_gpu_block(t, local, steps=20, warmup=3):
     beside the plugin reaction (plugins.ReactionManager over
     cdb_reaction_calc) on the box's cells: FP64, Vm and iStim fixed at the
     resting state, `steps` calls after `warmup`, CUDA events on each side's
-    launching stream.  The reference's GPU diffusion (CUDADiffusion) is not
-    run: its kernel returns from threads before a __syncthreads."""
+    launching stream.  The reference's GPU diffusion (CUDADiffusion) has
+    another stencil rule (6 faces, not FGR's 19 points) and runs only on y
+    and z extents that are multiples of 30, so it is timed apart
+    (reference_gpu_diffusion_block)."""
     from oracle import refgpu
     if not refgpu.available():
         return None
@@ -722,7 +726,48 @@ def reference_gpu_block(t, local, steps=20, warmup=3):
             "unit": METRIC, "steps": steps, "warmup": warmup, "dtype": "f64",
             "what": "reaction only (3 BetterTT06 types, Vm and iStim fixed): the reference's NVRTC kernel "
                     "through its ReactionManager::calc, built from its sources with USE_CUDA, against "
-                    "plugins.ReactionManager over cdb_reaction_calc; the reference's GPU diffusion is not run"}
+                    "plugins.ReactionManager over cdb_reaction_calc (the 6-face GPU diffusion: reference_gpu_diffusion)"}
+
+
+def reference_gpu_diffusion_block(local, steps=20, warmup=3):
+    """The reference's own "cuda" Diffusion on the GPU (CUDADiffusion with
+    diff_6face_v1, oracle/_ref/ref_gpu_diff6, in a child process) beside the
+    6-face plugin (plugins.CUDADiffusion over cdb_diff6_*): one
+    updateLocalVoltage + calc per step, FP64, on a 128 x 120 x 120 box (y
+    and z extents multiples of 30, the shapes on which the reference kernel
+    reaches every barrier), CUDA events on each side's launching stream; the
+    largest difference of the two dVm, relative to the largest |dVm|."""
+    from oracle import refgpu
+    if not refgpu.diff6_available():
+        return None
+    import torch
+    from cardioid_b200 import plugins, tissue
+    t = tissue.box(128, 120, 120, seed=1234)
+    ref_dvm, info = refgpu.diff6(t, t.vm0, t.diffusion_scale, steps=steps)
+    d = plugins.CUDADiffusion(t, t.diffusion_scale, device=local)
+    V = torch.tensor(t.vm0, device="cuda:%d" % local)
+    out = torch.empty_like(V)
+    for _ in range(warmup):
+        d.updateLocalVoltage(V)
+        d.calc(out)
+    torch.cuda.synchronize(local)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    for _ in range(steps):
+        d.updateLocalVoltage(V)
+        d.calc(out)
+    s1.record()
+    s1.synchronize()
+    ms = s0.elapsed_time(s1) / steps
+    got = out.cpu().numpy()
+    d.close()
+    ours = {"value": t.n / (ms / 1e3), "ms_per_step": ms}
+    ref = {"value": t.n / (info["ms_per_step"] / 1e3), "ms_per_step": info["ms_per_step"]}
+    return {"reference": ref, "ours_plugin": ours, "ours_over_reference": ours["value"] / ref["value"],
+            "unit": METRIC, "steps": steps, "warmup": warmup, "dtype": "f64", "cells": t.n,
+            "max_rel_diff_dvm": float(np.abs(got - ref_dvm).max() / np.abs(ref_dvm).max()),
+            "what": "6-face (\"cuda\") diffusion only, 128x120x120 box: the reference's CUDADiffusion (diff_6face_v1, "
+                    "map_dVm, copy_to_block) built from its sources, against plugins.CUDADiffusion over cdb_diff6_*"}
 
 
 def run_reference(args):

@@ -14,11 +14,13 @@
 // oracle/_ref/ref_gpu_diff6 by oracle/ref/Makefile; the product never links
 // or runs it.
 //
-// Usage: ref_gpu_diff6 NX NY NZ DX DY DZ SCALE GIDS CELLTYPES SIGMA VM OUT
+// Usage: ref_gpu_diff6 NX NY NZ DX DY DZ SCALE GIDS CELLTYPES SIGMA VM OUT [STEPS]
 //   GIDS int64 gid per cell (gid = x + nx (y + ny z)), CELLTYPES int32,
 //   SIGMA float64 [n][6] (a11 a12 a13 a22 a23 a33), VM float64 [n], all
 //   binary; OUT receives dVm (float64 [n]) from one updateLocalVoltage +
-//   calc, as the reference's omp loop calls them.
+//   calc, as the reference's omp loop calls them.  With STEPS, that pair is
+//   then timed STEPS times (CUDA events on the default stream, after 3
+//   untimed pairs) and one JSON line gives ms per pair.
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -56,8 +58,8 @@ bool readFile(const char* path, void* dst, size_t bytes)
 
 int main(int argc, char** argv)
 {
-   if (argc != 13) {
-      std::fprintf(stderr, "usage: %s NX NY NZ DX DY DZ SCALE GIDS CELLTYPES SIGMA VM OUT\n", argv[0]);
+   if (argc != 13 && argc != 14) {
+      std::fprintf(stderr, "usage: %s NX NY NZ DX DY DZ SCALE GIDS CELLTYPES SIGMA VM OUT [STEPS]\n", argv[0]);
       return 2;
    }
    const int nx = std::atoi(argv[1]), ny = std::atoi(argv[2]), nz = std::atoi(argv[3]);
@@ -125,6 +127,26 @@ int main(int argc, char** argv)
       std::fwrite(d.raw(), 8, n, f);
    }
    std::fclose(f);
-   std::printf("{\"cells\": %ld, \"grid\": [%d, %d, %d]}\n", n, grid.nx(), grid.ny(), grid.nz());
+   const int steps = argc == 14 ? std::atoi(argv[13]) : 0;
+   float ms = 0.f;
+   if (steps > 0) {
+      for (int k = 0; k < 3; ++k) {
+         diffusion.updateLocalVoltage(Vm);
+         diffusion.calc(dVm);
+      }
+      cudaEvent_t e0, e1;
+      if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return 3;
+      cudaDeviceSynchronize();
+      cudaEventRecord(e0, 0);
+      for (int k = 0; k < steps; ++k) {
+         diffusion.updateLocalVoltage(Vm);
+         diffusion.calc(dVm);
+      }
+      cudaEventRecord(e1, 0);
+      if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) return 3;
+      cudaEventElapsedTime(&ms, e0, e1);
+   }
+   std::printf("{\"cells\": %ld, \"grid\": [%d, %d, %d], \"steps\": %d, \"ms_per_step\": %.6f}\n", n, grid.nx(),
+               grid.ny(), grid.nz(), steps, steps > 0 ? ms / steps : 0.0);
    return 0;
 }

@@ -118,13 +118,14 @@ def diff6_available():
     return os.path.exists(DIFF6_BINARY)
 
 
-def diff6(t, vm, scale, timeout=300):
+def diff6(t, vm, scale, timeout=300, steps=0):
     """dVm from the reference's own "cuda" Diffusion on the GPU
     (oracle/_ref/ref_gpu_diff6: CUDADiffusion with diff_6face_v1, one
     updateLocalVoltage + calc as the omp loop calls them) for tissue t and
     Vm `vm`, diffusion scale `scale`.  t's extents in y and z must be
     multiples of 30 (the driver refuses other shapes: there the reference
-    kernel returns from threads before its barriers)."""
+    kernel returns from threads before its barriers).  With `steps`, also
+    returns the driver's JSON line (ms per updateLocalVoltage + calc)."""
     if not diff6_available():
         raise RuntimeError("oracle/_ref/ref_gpu_diff6 is not built (make -C oracle/ref gpu)")
     n = len(t.gid)
@@ -135,10 +136,14 @@ def diff6(t, vm, scale, timeout=300):
         np.ascontiguousarray(t.sigma, dtype=np.float64).reshape(-1).tofile(paths[2])
         np.ascontiguousarray(vm, dtype=np.float64).tofile(paths[3])
         cmd = [DIFF6_BINARY, str(t.nx), str(t.ny), str(t.nz), repr(t.dx), repr(t.dy), repr(t.dz), repr(scale)] + paths
+        if steps:
+            cmd.append(str(steps))
         res = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
         if res.returncode != 0:
             raise RuntimeError("ref_gpu_diff6 failed (%d): %s" % (res.returncode, res.stderr[-2000:]))
         out = np.fromfile(paths[4], dtype=np.float64)
     if out.size != n:
         raise RuntimeError("ref_gpu_diff6 wrote %d values, expected %d" % (out.size, n))
+    if steps:
+        return out, json.loads(res.stdout.strip().splitlines()[-1])
     return out
