@@ -8,9 +8,11 @@ use it.
 The face conductivities are pinned: tests/test_diff6.py checks face_sigma
 bit for bit against the table the reference's own CUDADiffusion
 constructor builds on the host (run by the oracle build, oracle/_ref).
-The flux is pinned only by restatement: the reference's kernel returns from
-threads before __syncthreads, so it is not run here; calc follows its code
-line by line.
+calc follows the kernel's code line by line.  The flux is pinned on the
+GPU (tests/test_diff6.py): the reference's kernel returns from threads
+before __syncthreads unless the local grid's y and z sizes are 30 k + 2,
+and on tissues of that shape the reference's own CUDADiffusion runs
+(oracle/_ref/ref_gpu_diff6) and both calc and the plugin match it.
 """
 import numpy as np
 
