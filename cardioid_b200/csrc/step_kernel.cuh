@@ -787,13 +787,14 @@ __global__ void __launch_bounds__(kCta, min_ctas<MIXED>()) fused_step_kernel(Ste
   int t = blockIdx.x * kWarpsPerCta + warpInCta;
   const TileWindow noWin{nullptr, nullptr, 0};
   if (!WIN && !a.stage) {
-    // the next tile's descriptor is in flight while this tile computes
-    WarpTile cur, nxt;
+    // the next tile's descriptor is in flight while this tile computes; a
+    // warp past its last tile takes an empty descriptor (never an
+    // uninitialised one, whose copy the compiler may treat as any value)
     EcgAcc ecg{ecgMine, -1, 0};
     MinMaxAcc mm{__longlong_as_double(0x7ff0000000000000ll), -__longlong_as_double(0x7ff0000000000000ll), -1};
-    if (t < a.nTiles) cur = a.tiles[t];
+    WarpTile cur = t < a.nTiles ? a.tiles[t] : WarpTile{};
     for (; t < a.nTiles; t += stride) {
-      if (t + stride < a.nTiles) nxt = a.tiles[t + stride];
+      const WarpTile nxt = t + stride < a.nTiles ? a.tiles[t + stride] : WarpTile{};
       step_tile<MIXED, SLOT, ECG, false>(a, cur, lane, nullptr, false, noWin, ecg, mm);
       cur = nxt;
     }
