@@ -901,11 +901,10 @@ cdb_status cdb_engine_create(const cdb_engine_config* cfg, cdb_engine** out)
   CDB_CUDA(cudaDeviceGetAttribute(&e->e.numSms, cudaDevAttrMultiProcessorCount, cfg->device));
   CDB_CUDA(e->e.dErr.alloc(sizeof(int)));
   CDB_CUDA(cudaMemset(e->e.dErr.p, 0, sizeof(int)));
-  // measured on the 256^3 box: bulk-copy staging is fastest for the mixed
-  // step (1.02 ms against 1.10 with cp.async); FP64 keeps direct loads
-  // defaults: the autotuner's choice on the 256^3 box (mixed: row tiles with
-  // their Vm window by TMA; FP64: direct loads)
-  e->e.stage = cfg->precision == CDB_MIXED ? 3 : 0;
+  // defaults, from the autotuner's tables on the 256^3 box (rows layout):
+  // mixed, bulk-copy staging (stage 2; 1-3 % ahead of stage 3's Vm windows
+  // and 6-8 % ahead of direct loads over five boxes); FP64, direct loads
+  e->e.stage = cfg->precision == CDB_MIXED ? 2 : 0;
   CDB_CUDA(cfg->precision == CDB_MIXED ? allow_step_smem<true>() : allow_step_smem<false>());
   *out = e.release();
   return CDB_OK;

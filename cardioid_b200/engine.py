@@ -227,7 +227,7 @@ class Engine:
         memory, 2 = bulk (TMA) copies into shared memory completing on an
         mbarrier, 3 = as 2, plus the Vm tile and halo of each row tile (the
         nine stencil rows of 32 consecutive voxels of a volume tissue) copied
-        into shared memory while the reaction computes (defaults: 3 mixed,
+        into shared memory while the reaction computes (defaults: 2 mixed,
         0 FP64; every stage gives the same bits); ctas_per_sm sizes the
         persistent grid (0: as many CTAs per SM as are resident)."""
         _lib.check(_lib.load().cdb_engine_set_tuning(self.h, int(stage), int(ctas_per_sm)))

@@ -312,7 +312,7 @@ cdb_status cdb_diag_fit_forms(const cdb_fit fits[CDB_NUM_FITS], int32_t poolSize
  * loads; ctasPerSm sizes the
  * persistent grid (SMs x ctasPerSm CTAs of 128 threads), 0 = as many CTAs as
  * are resident on an SM at once.  All stages give the same results bit for
- * bit.  Defaults: stage 3 for CDB_MIXED, 0 for CDB_FP64, ctasPerSm 0;
+ * bit.  Defaults: stage 2 for CDB_MIXED, 0 for CDB_FP64, ctasPerSm 0;
  * cardioid_b200.autotune picks them by timing. */
 cdb_status cdb_engine_set_tuning(cdb_engine* e, int32_t stage, int32_t ctasPerSm);
 cdb_status cdb_engine_get_tuning(cdb_engine* e, int32_t* stage, int32_t* ctasPerSm);
