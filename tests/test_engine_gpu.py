@@ -467,15 +467,19 @@ def test_non_finite_vm_reported_by_sync(cdb_lib, fits002):
         e.sync()
 
 
-def test_bounded_wait_runs_out_and_engine_recovers(cdb_lib, fits002):
+@pytest.mark.parametrize("stage", [2, 3])
+def test_bounded_wait_runs_out_and_engine_recovers(cdb_lib, fits002, stage):
     """The failure path of the step's bounded waits, made without a fault:
     one batch withholds its bulk copies after each warp's first tile (a wait
     that nothing completes), its waits give up after about a second, the
     warps leave, and cdb_engine_sync reports CDB_TIMEOUT; the next batches
-    run normally on the same context."""
+    run normally on the same context.  Bulk-copy staging (2) and the same
+    with the Vm windows of row tiles (3)."""
     from cardioid_b200 import _lib
     t = tissue.box(96, 96, 96)          # about 9000 tiles per type: several per warp
     with eng_mod.Engine(DT, precision="mixed") as e:
+        e.set_tuning(stage, 0)
+        e.set_layout("rows")
         rx, _ = eng_mod.transmural_setup(e, t, DT)
         tid = e.add_tissue(t, rx)
         e.step(5)
