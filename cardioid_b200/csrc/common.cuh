@@ -155,31 +155,89 @@ inline bool spec_pool32(const double* pool, float* out, int poolSize)
   return true;
 }
 
-// How the compiled mixed kernels evaluate fit f in FP32: Horner (shifted
-// fits, in t; fits of Ca_ss or V - E_K as written), or the power basis (sum
-// of c_k V^k with V^k by repeated products, low terms first) for the other
-// fits of V.
-inline bool spec_horner32(int f) { return ((kSpecShiftMask >> f) & 1u) || f == 0 || f == 29; }
-
 // One fit's FP32 numerator or denominator polynomial (n coefficients,
-// c[0] the constant term), evaluated in the kernel's order.
-inline float spec_poly32(const float* c, int n, float x, bool horner)
+// c[0] the constant term) as the compiled mixed kernels evaluate it: Horner
+// with one rounding per step (fit_pair32 runs the numerator's and the
+// denominator's chains in the two lanes of one FMA, each lane rounded as
+// fmaf, so each chain's value is this one).
+inline float spec_poly32(const float* c, int n, float x)
 {
-  if (horner) {
-    float r = c[n - 1];
-    for (int k = n - 2; k >= 0; --k) r = std::fma(x, r, c[k]);
-    return r;
-  }
-  float r = c[0], p = 1.0f;
-  for (int k = 1; k < n; ++k) {
-    p = p * x;
-    r = std::fma(p, c[k], r);
-  }
+  float r = c[n - 1];
+  for (int k = n - 2; k >= 0; --k) r = std::fma(x, r, c[k]);
   return r;
 }
 
+// The paired FP32 pool of the compiled mixed kernels (fit_pair32's layout,
+// tt06_device.cuh) from the FP32 pool at the compiled offsets
+// (spec_pool32); out holds at least kPairPool floats, zero outside the
+// fits' blocks.
+inline void spec_pair_pool32(const float* spec32, float* out, int outSize)
+{
+  for (int k = 0; k < outSize; ++k) out[k] = 0.0f;
+  for (int f = 0; f < kNumFits; ++f) {
+    const int O = kSpecOffset[f], N = kSpecNumer[f], D = kSpecDenom[f], B = pair_offset(f);
+    const int L = pair_lead(f), S = pair_steps(f), P0 = pair_first(f);
+    // coefficient of step i of the numerator chain (top first), and of
+    // step j of the denominator chain (its last step adds the form's 1)
+    auto num = [&](int i) { return spec32[O + N - 2 - i]; };
+    auto den = [&](int j) { return j < D - 2 ? spec32[O + N + D - 3 - j] : 1.0f; };
+    out[B] = spec32[O + N - 1];
+    if (D == 1) {
+      for (int i = 0; i < L; ++i) out[B + 2 + i] = num(i);
+      continue;
+    }
+    out[B + 1] = spec32[O + N + D - 2];
+    for (int i = 0; i < L; ++i) out[B + 2 + i] = N > D ? num(i) : den(i);
+    const int i0 = N > D ? L : 0, j0 = N > D ? 0 : L;
+    for (int k = 0; k < S; ++k) {
+      out[B + P0 + 2 * k] = num(i0 + k);
+      out[B + P0 + 2 * k + 1] = den(j0 + k);
+    }
+  }
+}
+static_assert(kPairPool <= kFitPoolPerType, "the paired pool exceeds the per-type pool");
+
+// Whether the paired pool gives every fit's numerator and denominator the
+// same values, bit for bit, as the Horner chains of spec_poly32 on the
+// FP32 pool, at 41 points of each fit's domain: fit_pair32's steps
+// restated on the host, one std::fma per lane (a check of the layout).
+inline bool spec_pair_ok(const float* spec32, const float* paired)
+{
+  float dc[CDB_MAX_COEFF + 1];
+  for (int f = 0; f < kNumFits; ++f) {
+    const int O = kSpecOffset[f], N = kSpecNumer[f], D = kSpecDenom[f], B = pair_offset(f);
+    const int L = pair_lead(f), S = pair_steps(f), P0 = pair_first(f);
+    const bool shifted = (kSpecShiftMask >> f) & 1u;
+    dc[0] = 1.0f;
+    for (int k = 1; k < D; ++k) dc[k] = spec32[O + N + k - 1];
+    const double lo = f == 0 ? 1e-7 : -100.0, hi = f == 0 ? 0.1 : 100.0;
+    for (int i = 0; i <= 40; ++i) {
+      const double xd = lo + (hi - lo) * i / 40;
+      const float x = shifted ? std::fma((float)xd, 1.0f / kSpecShiftScale, -kSpecShift[f] / kSpecShiftScale)
+                              : (float)xd;
+      float num = paired[B], den = 1.0f;
+      if (D == 1) {
+        for (int k = 0; k < L; ++k) num = std::fma(x, num, paired[B + 2 + k]);
+      } else {
+        den = paired[B + 1];
+        for (int k = 0; k < L; ++k) {
+          if (N > D) num = std::fma(x, num, paired[B + 2 + k]);
+          else den = std::fma(x, den, paired[B + 2 + k]);
+        }
+        for (int k = 0; k < S; ++k) {
+          num = std::fma(x, num, paired[B + P0 + 2 * k]);
+          den = std::fma(x, den, paired[B + P0 + 2 * k + 1]);
+        }
+      }
+      const float wn = spec_poly32(spec32 + O, N, x), wd = D > 1 ? spec_poly32(dc, D, x) : 1.0f;
+      if (std::memcmp(&num, &wn, sizeof(float)) != 0 || std::memcmp(&den, &wd, sizeof(float)) != 0) return false;
+    }
+  }
+  return true;
+}
+
 // Whether the FP32 forms of spec_pool32, evaluated as the mixed kernels do
-// (spec_horner32 / spec_poly32, FP32 quotient), stay within 1e-5 of each
+// (spec_poly32, FP32 quotient), stay within 1e-5 of each
 // fit's largest magnitude against the FP64 monomial form over the fit's
 // domain (V in [-100, 100] mV; Ca_ss in [1e-7, 0.1] mM for slot 0).
 inline bool spec_fp32_ok(const double* pool, const float* pool32)
@@ -187,7 +245,7 @@ inline bool spec_fp32_ok(const double* pool, const float* pool32)
   float dc[CDB_MAX_COEFF + 1];
   for (int f = 0; f < kNumFits; ++f) {
     const int O = kSpecOffset[f], N = kSpecNumer[f], D = kSpecDenom[f];
-    const bool shifted = (kSpecShiftMask >> f) & 1u, horner = spec_horner32(f);
+    const bool shifted = (kSpecShiftMask >> f) & 1u;
     dc[0] = 1.0f;
     for (int k = 1; k < D; ++k) dc[k] = pool32[O + N + k - 1];
     const double lo = f == 0 ? 1e-7 : -100.0, hi = f == 0 ? 0.1 : 100.0;
@@ -206,7 +264,7 @@ inline bool spec_fp32_ok(const double* pool, const float* pool32)
       const double v = num / den;
       const float xf = shifted ? std::fma((float)x, 1.0f / kSpecShiftScale, -kSpecShift[f] / kSpecShiftScale)
                                : (float)x;
-      const float vf = spec_poly32(pool32 + O, N, xf, horner) / spec_poly32(dc, D, xf, horner);
+      const float vf = spec_poly32(pool32 + O, N, xf) / spec_poly32(dc, D, xf);
       maxVal = std::max(maxVal, std::fabs(v));
       const double e = std::fabs((double)vf - v);
       maxErr = std::isfinite(e) ? std::max(maxErr, e) : 1e300;
@@ -217,8 +275,9 @@ inline bool spec_fp32_ok(const double* pool, const float* pool32)
 }
 
 // Packs 30 fits at the compile-time offsets of fit_shapes.h, zero-padded,
-// when every fit is no longer than the compiled shape and the mixed
-// kernels' FP32 forms of them are accurate (spec_fp32_ok); false otherwise.
+// when every fit is no longer than the compiled shape, the mixed kernels'
+// FP32 forms of them are accurate (spec_fp32_ok) and their paired pool
+// reproduces those forms (spec_pair_ok); false otherwise.
 inline bool pack_fits_spec(const cdb_fit* fits, double* pool, int poolSize)
 {
   static_assert(kSpecPool <= kFitPoolPerType, "compiled fit pool exceeds the per-type pool");
@@ -234,8 +293,10 @@ inline bool pack_fits_spec(const cdb_fit* fits, double* pool, int poolSize)
     for (int k = 0; k < nn; ++k) pool[O + k] = fits[f].coeff[k];
     for (int k = 0; k < nd - 1; ++k) pool[O + N + k] = fits[f].coeff[nn + k];
   }
-  std::vector<float> pool32(poolSize);
-  return spec_pool32(pool, pool32.data(), poolSize) && spec_fp32_ok(pool, pool32.data());
+  std::vector<float> pool32(poolSize), paired(poolSize);
+  if (!spec_pool32(pool, pool32.data(), poolSize) || !spec_fp32_ok(pool, pool32.data())) return false;
+  spec_pair_pool32(pool32.data(), paired.data(), poolSize);
+  return spec_pair_ok(pool32.data(), paired.data());
 }
 
 inline TT06Scalars to_scalars(const cdb_tt06_params& p)

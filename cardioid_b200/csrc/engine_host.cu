@@ -144,9 +144,15 @@ int acquire_slot(int device, const TT06Scalars& scal, const FitShape& shape, con
     }
   for (int s = 0; s < CDB_MAX_REACTION_TYPES; ++s) {
     if (used[s].refs > 0) continue;
-    // the compiled kernels' FP32 forms (shifted fits) for a specialised pool
+    // the compiled kernels' FP32 forms (shifted fits) for a specialised
+    // pool, in the paired layout of fit_pair32
     std::vector<float> pool32(pool.begin(), pool.end());
-    if (spec && !spec_pool32(pool.data(), pool32.data(), (int)pool.size())) return -1;
+    if (spec) {
+      if (!spec_pool32(pool.data(), pool32.data(), (int)pool.size())) return -1;
+      std::vector<float> paired(pool32.size());
+      spec_pair_pool32(pool32.data(), paired.data(), (int)paired.size());
+      pool32.swap(paired);
+    }
     err = cudaMemcpyToSymbol(c_scal, &scal, sizeof(scal), s * sizeof(TT06Scalars));
     if (err == cudaSuccess) err = cudaMemcpyToSymbol(c_shape, &shape, sizeof(shape), s * sizeof(FitShape));
     if (err == cudaSuccess)

@@ -163,7 +163,7 @@ struct IndexCheck {
 __constant__ TT06Scalars c_scal[CDB_MAX_REACTION_TYPES];
 __constant__ FitShape c_shape[CDB_MAX_REACTION_TYPES];
 __constant__ double c_coef64[CDB_MAX_REACTION_TYPES * kFitPoolPerType];
-__constant__ float c_coef32[CDB_MAX_REACTION_TYPES * kFitPoolPerType];
+__constant__ __align__(16) float c_coef32[CDB_MAX_REACTION_TYPES * kFitPoolPerType];   // paired layout for compiled slots (fit_pair32)
 
 // AoSoA row sizes
 constexpr int kRows64 = kNumStates;                 // FP64 state rows

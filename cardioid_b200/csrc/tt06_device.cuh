@@ -15,10 +15,12 @@
 //          concentrations in FP64 (their per-step increments are ~1e-7 of
 //          their values).  The compiled kernels evaluate the few fits whose
 //          monomial form loses accuracy in FP32 in a shifted argument
-//          (fit_shift32); the generic kernel evaluates them in FP64.
+//          (fit_form32); the generic kernel evaluates them in FP64.
 // Fit evaluation is a policy: GenericFits reads term counts at run time;
 // SpecFits has them as compile-time constants (fit_shapes.h), so every
-// Horner chain unrolls and the 30 independent chains interleave.
+// Horner chain unrolls and the 30 independent chains interleave; its FP32
+// fits run each numerator and denominator chain pair in two-lane FMAs
+// (fit_pair32).
 #pragma once
 #include <cstdint>
 
@@ -164,72 +166,104 @@ __device__ __forceinline__ double fit_spec64(const double* __restrict__ c, doubl
   return div64(num, den);
 }
 
-template <int SLOT>
-__device__ __forceinline__ float fit_spec32(const float* __restrict__ c, float x)
-{
-  constexpr int N = kSpecNumer[SLOT], D = kSpecDenom[SLOT], O = kSpecOffset[SLOT];
-  float num = c[O + N - 1];
-#pragma unroll
-  for (int k = N - 2; k >= 0; --k) num = fmaf(x, num, c[O + k]);
-  if (D == 1) return num;
-  float den = c[O + N + D - 2];
-#pragma unroll
-  for (int k = D - 3; k >= 0; --k) den = fmaf(x, den, c[O + N + k]);
-  den = fmaf(x, den, 1.0f);
-  return fdiv(num, den);
-}
-
-// FP32 fits of V in the power basis: with pw[k] = V^k computed once per
-// cell (shared by every V-fit), each term is fma(pw[k], c_k, acc), so the
-// coefficient is the multiplicand and can be an immediate constant-bank
-// operand; Horner's form puts it in the addend slot, where it needs a load.
-// Used only for the fits the FP32 error check accepted as written (well
-// conditioned in the monomial basis, so the two summation orders agree to
-// FP32 rounding).
-constexpr int kMaxPow = 24;
-
-template <int SLOT, int P>
-__device__ __forceinline__ float fit_pow32(const float* __restrict__ c, const float (&pw)[P])
-{
-  constexpr int N = kSpecNumer[SLOT], D = kSpecDenom[SLOT], O = kSpecOffset[SLOT];
-  static_assert(N <= P && D <= P, "power table too short");
-  float num = c[O];
-#pragma unroll
-  for (int k = 1; k < N; ++k) num = fmaf(pw[k], c[O + k], num);
-  if (D == 1) return num;
-  float den = fmaf(pw[1], c[O + N], 1.0f);
-#pragma unroll
-  for (int k = 2; k < D; ++k) den = fmaf(pw[k], c[O + N + k - 1], den);
-  return fdiv(num, den);
-}
-
-// FP32 fit in the shifted argument t = (x - s) / h of fit_shapes.h (the
-// fits whose monomial form loses accuracy in FP32: their numerator and
-// denominator span many decades over the domain, and about the shift point
-// the Taylor coefficients no longer cancel), by Horner in t.  h is a power
-// of two, so t is one FMA with immediate operands and no extra rounding;
-// the coefficients were rewritten in t at registration (spec_pool32).
-// (The power basis of t, with a power table per shift, measured slower:
-// its products cost more than Horner's chains.)
-template <int SLOT>
-__device__ __forceinline__ float fit_shift32(const float* __restrict__ c, float x)
-{
-  constexpr float inv = 1.0f / kSpecShiftScale, off = -kSpecShift[SLOT] / kSpecShiftScale;
-  return fit_spec32<SLOT>(c, fmaf(x, inv, off));
-}
-
 __host__ __device__ constexpr bool spec_shifted(int slot) { return (kSpecShiftMask >> slot) & 1u; }
 
-// The largest power any power-basis V-fit of the compiled shapes needs.
-__host__ __device__ constexpr int spec_max_pow32()
+// ---- the compiled mixed kernels' FP32 fits: paired Horner chains ----
+//
+// A rational fit num(x) / (1 + x den'(x)) is two Horner chains in the same
+// argument, num <- fma(x, num, c) and den <- fma(x, den, d), independent
+// of each other.  sm_100's two-lane FP32 FMA (__ffma2_rn, each lane rounded
+// as fmaf) takes one step of both, so the chains run together for as many
+// steps as the shorter one has, after the longer one's first steps run
+// alone: one instruction per pair of FMAs, with the same operations and
+// rounding as the two scalar chains.  Every fit runs this way: the fits in
+// kSpecShiftMask in the shifted argument t = (x - s) / h of fit_shapes.h
+// (their monomial form loses accuracy in FP32: numerator and denominator
+// span many decades over the domain, and about the shift point the Taylor
+// coefficients no longer cancel; h is a power of two, so t is one FMA with
+// immediate operands and no extra rounding; registration rewrote their
+// coefficients in t, spec_pool32), the others as written.
+//
+// Pool layout (built at registration from the FP32 pool, spec_pair_pool32):
+// per fit an even-aligned block holding the numerator's and the
+// denominator's top coefficients, the coefficients of the longer chain's
+// lone steps (top first), padding to an even index, then one (numerator,
+// denominator) coefficient pair per joint step; the denominator's last
+// coefficient is the 1 of its form 1 + x (...).  A polynomial fit
+// (denominator 1) holds its top coefficient, one pad and its remaining
+// coefficients, top first.
+// The layout per fit, for the device (compile-time F) and for the host
+// (run-time f, spec_pair_pool32); the two agree (static_assert below).
+template <int F>
+struct PairShape {
+  static constexpr int N = kSpecNumer[F], D = kSpecDenom[F];
+  static constexpr int steps = D == 1 ? 0 : (N < D ? N : D) - 1;          // joint steps
+  static constexpr int lead = D == 1 ? N - 1 : (N > D ? N : D) - 1 - steps;   // lone steps of the longer chain
+  static constexpr int first = (2 + lead + 1) & ~1;                        // first pair, in the block
+  static constexpr int block = first + 2 * steps;
+};
+template <int F>
+struct PairOffset {
+  static constexpr int value = PairOffset<F - 1>::value + PairShape<F - 1>::block;
+};
+template <>
+struct PairOffset<0> {
+  static constexpr int value = 0;
+};
+constexpr int kPairPool = PairOffset<30>::value;
+
+constexpr int pair_steps(int f)
 {
-  int m = 1;
-  for (int s = 1; s < 30; ++s) {
-    if (s == 29 || spec_shifted(s)) continue;   // K1 takes V - E_K; shifted fits use Horner in t
-    const int need = kSpecNumer[s] > kSpecDenom[s] ? kSpecNumer[s] : kSpecDenom[s];
-    if (need > m) m = need;
+  return kSpecDenom[f] == 1 ? 0 : (kSpecNumer[f] < kSpecDenom[f] ? kSpecNumer[f] : kSpecDenom[f]) - 1;
+}
+constexpr int pair_lead(int f)
+{
+  return kSpecDenom[f] == 1 ? kSpecNumer[f] - 1
+                            : (kSpecNumer[f] > kSpecDenom[f] ? kSpecNumer[f] : kSpecDenom[f]) - 1 - pair_steps(f);
+}
+constexpr int pair_first(int f) { return (2 + pair_lead(f) + 1) & ~1; }
+constexpr int pair_offset(int f)
+{
+  int o = 0;
+  for (int g = 0; g < f; ++g) o += pair_first(g) + 2 * pair_steps(g);
+  return o;
+}
+static_assert(pair_offset(30) == kPairPool && pair_offset(29) == PairOffset<29>::value &&
+                  pair_offset(13) == PairOffset<13>::value,
+              "host and device pool layouts agree");
+
+// FP32 fit F of the paired pool c (8-byte aligned) at argument x.
+template <int F>
+__device__ __forceinline__ float fit_pair32(const float* __restrict__ c, float x)
+{
+  constexpr int N = kSpecNumer[F], D = kSpecDenom[F], B = PairOffset<F>::value;
+  constexpr int L = PairShape<F>::lead, S = PairShape<F>::steps, P0 = PairShape<F>::first;
+  if (D == 1) {
+    float num = c[B];
+#pragma unroll
+    for (int i = 0; i < L; ++i) num = fmaf(x, num, c[B + 2 + i]);
+    return num;
   }
-  return m;
+  float num = c[B], den = c[B + 1];
+#pragma unroll
+  for (int i = 0; i < L; ++i) {
+    if (N > D) num = fmaf(x, num, c[B + 2 + i]);
+    else den = fmaf(x, den, c[B + 2 + i]);
+  }
+  float2 nd = make_float2(num, den);
+  const float2 xx = make_float2(x, x);
+#pragma unroll
+  for (int k = 0; k < S; ++k) nd = __ffma2_rn(xx, nd, *reinterpret_cast<const float2*>(c + B + P0 + 2 * k));
+  return fdiv(nd.x, nd.y);
+}
+
+// The same in the fit's shifted argument when it has one.
+template <int F>
+__device__ __forceinline__ float fit_form32(const float* __restrict__ c, float x)
+{
+  if (!spec_shifted(F)) return fit_pair32<F>(c, x);
+  constexpr float inv = 1.0f / kSpecShiftScale, off = -kSpecShift[F] / kSpecShiftScale;
+  return fit_pair32<F>(c, fmaf(x, inv, off));
 }
 
 // Fit evaluation policies.  c64 / c32 point at one reaction type's
@@ -256,32 +290,17 @@ struct GenericFits {
 
 struct SpecFits {
   const double* __restrict__ c64;
-  const float* __restrict__ c32;
-  float pw[kMaxPow];   // V^k for the power-basis V-fits (set_v)
-  float v;             // V in FP32 (set_v)
-  __device__ __forceinline__ void set_v(float vf)
-  {
-    v = vf;
-    pw[0] = 1.0f;
-#pragma unroll
-    for (int k = 1; k < spec_max_pow32(); ++k) pw[k] = pw[k - 1] * vf;
-  }
+  const float* __restrict__ c32;   // the paired FP32 pool (fit_pair32)
+  float v;                         // V in FP32 (set_v)
+  __device__ __forceinline__ void set_v(float vf) { v = vf; }
   template <int SLOT>
   __device__ __forceinline__ double f64(double x) const { return fit_spec64<SLOT>(c64, x); }
-  // a fit of another argument (Ca_ss, V - E_K): Horner in x or in t
+  // a fit of another argument (Ca_ss, V - E_K)
   template <int SLOT>
-  __device__ __forceinline__ float fmix(float xf, double) const
-  {
-    if (spec_shifted(SLOT)) return fit_shift32<SLOT>(c32, xf);
-    return fit_spec32<SLOT>(c32, xf);
-  }
-  // a fit of V: the power basis, or Horner in t for the shifted fits
+  __device__ __forceinline__ float fmix(float xf, double) const { return fit_form32<SLOT>(c32, xf); }
+  // a fit of V
   template <int SLOT>
-  __device__ __forceinline__ float fv(double) const
-  {
-    if (spec_shifted(SLOT)) return fit_shift32<SLOT>(c32, v);
-    return fit_pow32<SLOT>(c32, pw);
-  }
+  __device__ __forceinline__ float fv(double) const { return fit_form32<SLOT>(c32, v); }
 };
 
 struct ConstsD {

@@ -63,11 +63,12 @@ def _pow32(c, x):
 
 
 def horner_slot(slot):
-    """The fits the compiled mixed kernels evaluate by Horner when not
-    shifted (arguments other than V: Ca_ss for slot 0, V - E_K for slot
-    29); the other fits of V in the power basis; every shifted fit by
-    Horner in the shifted argument."""
-    return slot in (0, 29)
+    """Whether the compiled mixed kernels evaluate fit `slot` by Horner when
+    it is not shifted: every fit (fit_pair32 runs each numerator and
+    denominator chain pair by Horner in two-lane FMAs; a shifted fit runs
+    the same in the shifted argument).  _pow32 remains for comparing the
+    power basis."""
+    return True
 
 
 def _poly64(c, x):
