@@ -185,13 +185,15 @@ __host__ __device__ constexpr bool spec_shifted(int slot) { return (kSpecShiftMa
 // coefficients in t, spec_pool32), the others as written.
 //
 // Pool layout (built at registration from the FP32 pool, spec_pair_pool32):
-// per fit an even-aligned block holding the numerator's and the
+// per fit a 16-byte aligned block holding the numerator's and the
 // denominator's top coefficients, the coefficients of the longer chain's
-// lone steps (top first), padding to an even index, then one (numerator,
-// denominator) coefficient pair per joint step; the denominator's last
-// coefficient is the 1 of its form 1 + x (...).  A polynomial fit
-// (denominator 1) holds its top coefficient, one pad and its remaining
-// coefficients, top first.
+// lone steps (top first), padding to a 16-byte boundary, then one
+// (numerator, denominator) coefficient pair per joint step, two per
+// 16-byte load; the denominator's last coefficient is the 1 of its form
+// 1 + x (...).  A polynomial fit (denominator 1) holds its top coefficient,
+// one pad and its remaining coefficients, top first.  (16-byte pairs of
+// pairs measured 1 % faster on the 256^3 step than 8-byte pairs, same bits.)
+//
 // The layout per fit, for the device (compile-time F) and for the host
 // (run-time f, spec_pair_pool32); the two agree (static_assert below).
 template <int F>
@@ -199,8 +201,8 @@ struct PairShape {
   static constexpr int N = kSpecNumer[F], D = kSpecDenom[F];
   static constexpr int steps = D == 1 ? 0 : (N < D ? N : D) - 1;          // joint steps
   static constexpr int lead = D == 1 ? N - 1 : (N > D ? N : D) - 1 - steps;   // lone steps of the longer chain
-  static constexpr int first = (2 + lead + 1) & ~1;                        // first pair, in the block
-  static constexpr int block = first + 2 * steps;
+  static constexpr int first = (2 + lead + 3) & ~3;                        // first pair, 16-byte aligned
+  static constexpr int block = (first + 2 * steps + 3) & ~3;               // blocks start 16-byte aligned
 };
 template <int F>
 struct PairOffset {
@@ -221,18 +223,18 @@ constexpr int pair_lead(int f)
   return kSpecDenom[f] == 1 ? kSpecNumer[f] - 1
                             : (kSpecNumer[f] > kSpecDenom[f] ? kSpecNumer[f] : kSpecDenom[f]) - 1 - pair_steps(f);
 }
-constexpr int pair_first(int f) { return (2 + pair_lead(f) + 1) & ~1; }
+constexpr int pair_first(int f) { return (2 + pair_lead(f) + 3) & ~3; }
 constexpr int pair_offset(int f)
 {
   int o = 0;
-  for (int g = 0; g < f; ++g) o += pair_first(g) + 2 * pair_steps(g);
+  for (int g = 0; g < f; ++g) o += (pair_first(g) + 2 * pair_steps(g) + 3) & ~3;
   return o;
 }
 static_assert(pair_offset(30) == kPairPool && pair_offset(29) == PairOffset<29>::value &&
                   pair_offset(13) == PairOffset<13>::value,
               "host and device pool layouts agree");
 
-// FP32 fit F of the paired pool c (8-byte aligned) at argument x.
+// FP32 fit F of the paired pool c (16-byte aligned) at argument x.
 template <int F>
 __device__ __forceinline__ float fit_pair32(const float* __restrict__ c, float x)
 {
@@ -252,8 +254,14 @@ __device__ __forceinline__ float fit_pair32(const float* __restrict__ c, float x
   }
   float2 nd = make_float2(num, den);
   const float2 xx = make_float2(x, x);
+  // two joint steps' coefficient pairs per 16-byte load
 #pragma unroll
-  for (int k = 0; k < S; ++k) nd = __ffma2_rn(xx, nd, *reinterpret_cast<const float2*>(c + B + P0 + 2 * k));
+  for (int k = 0; k + 1 < S; k += 2) {
+    const float4 q = *reinterpret_cast<const float4*>(c + B + P0 + 2 * k);
+    nd = __ffma2_rn(xx, nd, make_float2(q.x, q.y));
+    nd = __ffma2_rn(xx, nd, make_float2(q.z, q.w));
+  }
+  if (S & 1) nd = __ffma2_rn(xx, nd, *reinterpret_cast<const float2*>(c + B + P0 + 2 * (S - 1)));
   return fdiv(nd.x, nd.y);
 }
 
