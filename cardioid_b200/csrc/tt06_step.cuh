@@ -122,7 +122,7 @@ template <class Fits, class IO>
 __device__ __forceinline__ float tt06_step_mixed(const TT06Scalars& p, const BlockScale& blk, Fits& fits,
                                                  float dtf, double V, IO& io)
 {
-  // every V-fit takes V (fv: the power basis where the policy has one)
+  // every V-fit takes V (fv: the policy evaluates it in V or in its shifted argument)
 #define FIT(slot, x) fits.template fv<slot>(V)
 #define FITX(slot, xf, xd) fits.template fmix<slot>(xf, xd)
   fits.set_v((float)V);
