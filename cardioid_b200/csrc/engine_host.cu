@@ -102,10 +102,11 @@ struct HostTissue {
   // Chunked host step (cdb_engine_step_host): chunk j holds cells
   // pipeCell[j] .. pipeCell[j+1]-1, whole planes of the slowest grid axis;
   // its compute launches take the tiles whose stencil needs no later chunk
-  // (per slot, local tiles up to pipeTiles[j][slot]); its new Vm is final
-  // once compute chunk pipeOut[j] has run.  pipeK = 1: one chunk.
+  // (per slot, local tiles up to pipeTiles[j][slot]).  Output range j,
+  // cells outCell[j] .. outCell[j+1]-1, is final once compute chunk
+  // pipeOut[j] has run.  pipeK = 1: one chunk.
   int pipeK = 1;
-  std::vector<int64_t> pipeCell;
+  std::vector<int64_t> pipeCell, outCell;
   std::vector<int> pipeOut;
   std::vector<std::array<int64_t, CDB_MAX_REACTION_TYPES>> pipeTiles;
 };
@@ -229,9 +230,29 @@ struct Engine {
 
   // copy streams and events of the chunked host step
   cudaStream_t sIn = nullptr, sOut = nullptr;
-  cudaEvent_t evStart = nullptr;
+  cudaEvent_t evStart = nullptr, evOut = nullptr;
   std::vector<cudaEvent_t> evIn, evComp;
   DeviceBuffer dStageOut;
+  // graphs of the chunked host step with page-locked host buffers, one per
+  // (Vm in, Vm out, parity): a time loop that alternates two buffers uses two
+  struct HostStepGraph {
+    const double* in;
+    double* out;
+    int parity;
+    cudaGraphExec_t exec;
+    int64_t launches;
+  };
+  std::vector<HostStepGraph> hostGraphs;
+
+  // Every captured graph goes whenever what it captured may change (tables,
+  // time table, tuning, staging buffers).
+  void drop_graphs()
+  {
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+    for (const HostStepGraph& g : hostGraphs) cudaGraphExecDestroy(g.exec);
+    hostGraphs.clear();
+  }
 
   cudaError_t ensure_pipe(int K)
   {
@@ -239,6 +260,7 @@ struct Engine {
     if (!sIn) err = cudaStreamCreateWithFlags(&sIn, cudaStreamNonBlocking);
     if (err == cudaSuccess && !sOut) err = cudaStreamCreateWithFlags(&sOut, cudaStreamNonBlocking);
     if (err == cudaSuccess && !evStart) err = cudaEventCreateWithFlags(&evStart, cudaEventDisableTiming);
+    if (err == cudaSuccess && !evOut) err = cudaEventCreateWithFlags(&evOut, cudaEventDisableTiming);
     while (err == cudaSuccess && (int)evIn.size() < K) {
       cudaEvent_t a = nullptr, b = nullptr;
       err = cudaEventCreateWithFlags(&a, cudaEventDisableTiming);
@@ -251,11 +273,12 @@ struct Engine {
 
   ~Engine()
   {
-    if (graph) cudaGraphExecDestroy(graph);
+    drop_graphs();
     tissues.clear();
     for (cudaEvent_t ev : evIn) cudaEventDestroy(ev);
     for (cudaEvent_t ev : evComp) cudaEventDestroy(ev);
     if (evStart) cudaEventDestroy(evStart);
+    if (evOut) cudaEventDestroy(evOut);
     if (sIn) cudaStreamDestroy(sIn);
     if (sOut) cudaStreamDestroy(sOut);
     if (stream) cudaStreamDestroy(stream);
@@ -291,7 +314,7 @@ struct Engine {
     CDB_CUDA(cudaStreamSynchronize(stream));
     CDB_CUDA(dTimes.alloc(all.size() * sizeof(double)));
     CDB_CUDA(cudaMemcpy(dTimes.p, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
-    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    drop_graphs();
     dirty = true;   // tissues' time offsets
     return CDB_OK;
   }
@@ -352,7 +375,7 @@ struct Engine {
       CDB_CUDA(cudaMemcpy(dTiles.p, tiles.data(), tiles.size() * sizeof(WarpTile), cudaMemcpyHostToDevice));
     if (!stims.empty())
       CDB_CUDA(cudaMemcpy(dStims.p, stims.data(), stims.size() * sizeof(cdb_stimulus), cudaMemcpyHostToDevice));
-    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    drop_graphs();
     dirty = false;
     return CDB_OK;
   }
@@ -622,6 +645,7 @@ void build_pipe(HostTissue& h, const int64_t* gid, const std::vector<int64_t>& c
 {
   h.pipeK = 1;
   h.pipeCell = {0, h.n};
+  h.outCell = {0, h.n};
   h.pipeOut = {0};
   h.pipeTiles.assign(1, {});
   for (int k = 0; k < CDB_MAX_REACTION_TYPES; ++k) h.pipeTiles[0][k] = (int64_t)h.tiles[k].size();
@@ -634,33 +658,47 @@ void build_pipe(HostTissue& h, const int64_t* gid, const std::vector<int64_t>& c
     stride = h.nx;
     planes = h.ny;
   }
-  // 16 chunks measured best on the 256^3 box (3.4 ms per step against 3.8
-  // with 8 and 3.7 with 32: more chunks shorten the pipeline's tail, fewer
-  // keep the step launches long)
-  const int K = (int)std::min<int64_t>(16, planes / 16);
-  if (K < 2 || n < (int64_t(1) << 16)) return;
+  // Chunks of planes/16 planes measured best on the 256^3 box (3.4 ms per
+  // step against 3.8 with planes/8 and 3.7 with planes/32: smaller chunks
+  // shorten the pipeline's head and tail, larger ones keep the step launches
+  // long); the first and the last are half as long (head and tail shorter
+  // again: 3.66 against 3.72 ms), so there are KF + 1 chunks.
+  const int KF = (int)std::min<int64_t>(16, planes / 16);
+  if (KF < 2 || n < (int64_t(1) << 16)) return;
+  const int K = KF + 1;
   auto g = [&](int64_t c) { return gid ? gid[c] : c; };
   for (int64_t c = 1; c < n; ++c)
     if (g(c) < g(c - 1)) return;
   auto plane = [&](int64_t c) { return g(c) / stride; };
   std::vector<int64_t> P(K + 1);   // chunk j: planes P[j] .. P[j+1]-1
-  for (int j = 0; j <= K; ++j) P[j] = j * planes / K;
-  auto chunk_of = [&](int64_t p) {
+  for (int j = 0; j <= K; ++j) P[j] = j == 0 ? 0 : j == K ? planes : (2 * j - 1) * planes / (2 * KF);
+  // Output range j: planes Q[j] .. Q[j+1]-1, one plane behind the chunks
+  // (a chunk's last plane waits for the next chunk's first), so compute
+  // chunk j completes output range j and its copy down starts a chunk
+  // earlier than chunk j's own would.
+  std::vector<int64_t> Q(K + 1);
+  for (int j = 0; j <= K; ++j) Q[j] = j == 0 || j == K ? P[j] : P[j] - 1;
+  auto range_of = [&](const std::vector<int64_t>& B, int64_t p) {
     int j = 0;
-    while (j + 1 < K && P[j + 1] <= p) ++j;
+    while (j + 1 < K && B[j + 1] <= p) ++j;
     return j;
   };
-  std::vector<int64_t> cells(K + 1, n);
-  for (int j = 0; j < K; ++j) {
-    int64_t lo = 0, hi = n;   // first cell with plane >= P[j]
-    while (lo < hi) {
-      const int64_t mid = (lo + hi) / 2;
-      if (plane(mid) >= P[j]) hi = mid;
-      else lo = mid + 1;
+  auto chunk_of = [&](int64_t p) { return range_of(P, p); };
+  auto first_cells = [&](const std::vector<int64_t>& B) {
+    std::vector<int64_t> cells(K + 1, n);
+    for (int j = 1; j < K; ++j) {
+      int64_t lo = 0, hi = n;   // first cell with plane >= B[j]
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) / 2;
+        if (plane(mid) >= B[j]) hi = mid;
+        else lo = mid + 1;
+      }
+      cells[j] = lo;
     }
-    cells[j] = lo;
-  }
-  cells[0] = 0;
+    cells[0] = 0;
+    return cells;
+  };
+  std::vector<int64_t> cells = first_cells(P), outCells = first_cells(Q);
   std::vector<int> out(K, 0);
   std::vector<std::array<int64_t, CDB_MAX_REACTION_TYPES>> ends(K);
   for (int k = 0; k < CDB_MAX_REACTION_TYPES; ++k) {
@@ -684,14 +722,15 @@ void build_pipe(HostTissue& h, const int64_t* gid, const std::vector<int64_t>& c
     for (const WarpTile& tl : h.tiles[k]) {
       const int r = req(tl);
       ++count[r];
-      for (int ch = chunk_of(plane(firstCell(tl))); ch <= chunk_of(plane(lastCell(tl))); ++ch)
-        out[ch] = std::max(out[ch], r);
+      for (int o = range_of(Q, plane(firstCell(tl))); o <= range_of(Q, plane(lastCell(tl))); ++o)
+        out[o] = std::max(out[o], r);
     }
     int64_t acc = 0;
     for (int j = 0; j < K; ++j) ends[j][k] = acc += count[j];
   }
   h.pipeK = K;
   h.pipeCell = std::move(cells);
+  h.outCell = std::move(outCells);
   h.pipeOut = std::move(out);
   h.pipeTiles = std::move(ends);
 }
@@ -926,10 +965,7 @@ cdb_status cdb_engine_set_tuning(cdb_engine* e, int32_t stage, int32_t ctasPerSm
   CDB_CUDA(cudaStreamSynchronize(E.stream));
   E.stage = stage;
   E.ctasPerSm = ctasPerSm;
-  if (E.graph) {
-    cudaGraphExecDestroy(E.graph);
-    E.graph = nullptr;
-  }
+  E.drop_graphs();
   return CDB_OK;
 }
 
@@ -1441,6 +1477,21 @@ cdb_status cdb_engine_read_weights(cdb_engine* e, int32_t id, double* host19)
   return CDB_OK;
 }
 
+// Whether n doubles at p lie in page-locked host memory (both ends: an
+// array is one allocation), which a captured copy needs.
+static bool host_locked(const void* p, int64_t n)
+{
+  cudaPointerAttributes a;
+  for (const void* q : {p, (const void*)((const double*)p + (n > 0 ? n - 1 : 0))}) {
+    if (cudaPointerGetAttributes(&a, q) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (a.type != cudaMemoryTypeHost) return false;
+  }
+  return true;
+}
+
 cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, double* vm_out)
 {
   NvtxRange range("cdb_engine_step_host");
@@ -1451,7 +1502,10 @@ cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, 
   CDB_CHECK(E.tissues.size() == 1, CDB_INVALID_ARG, "cdb_engine_step_host needs an engine with one tissue");
   CDB_CUDA(cudaSetDevice(E.cfg.device));
   const int64_t n = t->n;
-  if (E.dStage.bytes < (size_t)n * 8) CDB_CUDA(E.dStage.alloc(n * 8));
+  if (E.dStage.bytes < (size_t)n * 8) {
+    E.drop_graphs();
+    CDB_CUDA(E.dStage.alloc(n * 8));
+  }
   cudaStream_t s = E.stream;
   if (t->pipeK < 2) {
     const TissueDev& d = t->dev;
@@ -1475,14 +1529,20 @@ cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, 
   // the chunks whose new Vm is then final are gathered; a second copy
   // stream takes each of those down.  Both copy directions and the step
   // overlap, and every kernel stays on the engine's stream (the persistent
-  // step kernels hold every SM while they run).
+  // step kernels hold every SM while they run).  With page-locked host
+  // buffers the whole pattern (about ten API calls per chunk) is captured
+  // once as a graph and replayed by one launch, so the copies are queued at
+  // once instead of behind the host's issue of the chunks before them.
   cdb_status st = E.ensure_times(1);
   if (st != CDB_OK) return st;
   st = E.rebuild();
   if (st != CDB_OK) return st;
   const int K = t->pipeK;
   CDB_CUDA(E.ensure_pipe(K));
-  if (E.dStageOut.bytes < (size_t)n * 8) CDB_CUDA(E.dStageOut.alloc(n * 8));
+  if (E.dStageOut.bytes < (size_t)n * 8) {
+    E.drop_graphs();
+    CDB_CUDA(E.dStageOut.alloc(n * 8));
+  }
   const TissueDev& d = t->dev;
   double* const vin = d.vm[t->parity];
   double* const vout = d.vm[t->parity ^ 1];
@@ -1490,46 +1550,81 @@ cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, 
   t->dev.actAll = 1;
   double* const stIn = E.dStage.as<double>();
   double* const stOut = E.dStageOut.as<double>();
-  CDB_CUDA(cudaEventRecord(E.evStart, s));
-  CDB_CUDA(cudaStreamWaitEvent(E.sIn, E.evStart, 0));
-  CDB_CUDA(cudaStreamWaitEvent(E.sOut, E.evStart, 0));
-  for (int j = 0; j < K; ++j) {
-    const int64_t c0 = t->pipeCell[j], m = t->pipeCell[j + 1] - c0;
-    if (m > 0) CDB_CUDA(cudaMemcpyAsync(stIn + c0, vm_in + c0, m * 8, cudaMemcpyHostToDevice, E.sIn));
-    CDB_CUDA(cudaEventRecord(E.evIn[j], E.sIn));
+  auto enqueue = [&]() -> cudaError_t {
+    cudaError_t err = cudaEventRecord(E.evStart, s);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(E.sIn, E.evStart, 0);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(E.sOut, E.evStart, 0);
+    for (int j = 0; j < K && err == cudaSuccess; ++j) {
+      const int64_t c0 = t->pipeCell[j], m = t->pipeCell[j + 1] - c0;
+      if (m > 0) err = cudaMemcpyAsync(stIn + c0, vm_in + c0, m * 8, cudaMemcpyHostToDevice, E.sIn);
+      if (err == cudaSuccess) err = cudaEventRecord(E.evIn[j], E.sIn);
+    }
+    for (int j = 0; j < K && err == cudaSuccess; ++j) {
+      err = cudaStreamWaitEvent(s, E.evIn[j], 0);
+      if (err != cudaSuccess) break;
+      const int64_t c0 = t->pipeCell[j], m = t->pipeCell[j + 1] - c0;
+      if (m > 0) {
+        scatter_vm_kernel<<<grid_for(m, 256), 256, 0, s>>>(c0, m, stIn, vin, d.voxel, d.nx, d.ny, d.px, d.pxy, d.py0,
+                                                           d.pz0, flag);
+        E.launches += 1;
+      }
+      for (const auto& sl : E.slotTiles) {
+        const int64_t lo = j ? t->pipeTiles[j - 1][sl.first] : 0, hi = t->pipeTiles[j][sl.first];
+        if (hi > lo) E.launch_tiles(sl.first, sl.second.first + lo, hi - lo, 0, false, s);
+      }
+      bool down = false;
+      for (int i = 0; i < K; ++i) {
+        const int64_t g0 = t->outCell[i], gm = t->outCell[i + 1] - g0;
+        if (t->pipeOut[i] != j || gm == 0) continue;
+        gather_vm_kernel<<<grid_for(gm, 256), 256, 0, s>>>(g0, gm, vout, stOut, d.voxel, d.nx, d.ny, d.px, d.pxy,
+                                                           d.py0, d.pz0);
+        E.launches += 1;
+        down = true;
+      }
+      err = cudaEventRecord(E.evComp[j], s);
+      if (err == cudaSuccess && down) err = cudaStreamWaitEvent(E.sOut, E.evComp[j], 0);
+      // the chunks this compute chunk completed go down at once
+      for (int i = 0; i < K && err == cudaSuccess && down; ++i) {
+        const int64_t g0 = t->outCell[i], gm = t->outCell[i + 1] - g0;
+        if (t->pipeOut[i] != j || gm == 0) continue;
+        err = cudaMemcpyAsync(vm_out + g0, stOut + g0, gm * 8, cudaMemcpyDeviceToHost, E.sOut);
+      }
+    }
+    if (err != cudaSuccess) return err;
+    advance_kernel<<<1, 128, 0, s>>>(E.dTissues.as<TissueDev>(), 1, 1);
+    E.launches += 1;
+    err = cudaEventRecord(E.evOut, E.sOut);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(s, E.evOut, 0);
+    return err;
+  };
+  if (E.cfg.use_graphs && !E.withhold && host_locked(vm_in, n) && host_locked(vm_out, n)) {
+    Engine::HostStepGraph* g = nullptr;
+    for (Engine::HostStepGraph& h : E.hostGraphs)
+      if (h.in == vm_in && h.out == vm_out && h.parity == t->parity) g = &h;
+    if (!g) {
+      cudaGraph_t cg = nullptr;
+      CDB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      const int64_t before = E.launches;
+      const cudaError_t err = enqueue();
+      const int64_t per = E.launches - before;
+      E.launches = before;
+      const cudaError_t end = cudaStreamEndCapture(s, &cg);
+      CDB_CUDA(err);
+      CDB_CUDA(end);
+      cudaGraphExec_t exec = nullptr;
+      const cudaError_t inst = cudaGraphInstantiate(&exec, cg, 0);
+      cudaGraphDestroy(cg);
+      CDB_CUDA(inst);
+      E.hostGraphs.push_back(Engine::HostStepGraph{vm_in, vm_out, t->parity, exec, per});
+      g = &E.hostGraphs.back();
+    }
+    CDB_CUDA(cudaGraphLaunch(g->exec, s));
+    E.launches += g->launches;
+  } else {
+    CDB_CUDA(enqueue());
   }
-  for (int j = 0; j < K; ++j) {
-    CDB_CUDA(cudaStreamWaitEvent(s, E.evIn[j], 0));
-    const int64_t c0 = t->pipeCell[j], m = t->pipeCell[j + 1] - c0;
-    if (m > 0) {
-      scatter_vm_kernel<<<grid_for(m, 256), 256, 0, s>>>(c0, m, stIn, vin, d.voxel, d.nx, d.ny, d.px, d.pxy, d.py0,
-                                                         d.pz0, flag);
-      E.launches += 1;
-    }
-    for (const auto& sl : E.slotTiles) {
-      const int64_t lo = j ? t->pipeTiles[j - 1][sl.first] : 0, hi = t->pipeTiles[j][sl.first];
-      if (hi > lo) E.launch_tiles(sl.first, sl.second.first + lo, hi - lo, 0, false, s);
-    }
-    for (int i = 0; i < K; ++i) {
-      const int64_t g0 = t->pipeCell[i], gm = t->pipeCell[i + 1] - g0;
-      if (t->pipeOut[i] != j || gm == 0) continue;
-      gather_vm_kernel<<<grid_for(gm, 256), 256, 0, s>>>(g0, gm, vout, stOut, d.voxel, d.nx, d.ny, d.px, d.pxy, d.py0,
-                                                         d.pz0);
-      E.launches += 1;
-    }
-    CDB_CUDA(cudaEventRecord(E.evComp[j], s));
-  }
-  advance_kernel<<<1, 128, 0, s>>>(E.dTissues.as<TissueDev>(), 1, 1);
-  E.launches += 1;
   E.advance_host(1);
-  for (int j = 0; j < K; ++j) {
-    const int64_t c0 = t->pipeCell[j], m = t->pipeCell[j + 1] - c0;
-    if (m == 0) continue;
-    CDB_CUDA(cudaStreamWaitEvent(E.sOut, E.evComp[t->pipeOut[j]], 0));
-    CDB_CUDA(cudaMemcpyAsync(vm_out + c0, stOut + c0, m * 8, cudaMemcpyDeviceToHost, E.sOut));
-  }
   CDB_CUDA(cudaGetLastError());
-  CDB_CUDA(cudaStreamSynchronize(E.sOut));
   CDB_CUDA(cudaStreamSynchronize(s));
   return CDB_OK;
 }

@@ -746,9 +746,10 @@ __device__ __forceinline__ bool step_tile(const StepArgs& a, const WarpTile& til
 // Resident CTAs per SM the register budget aims at: 4 for FP64 (16 warps,
 // at most 128 registers) and 5 for mixed (20 warps, at most 102 registers,
 // which its shared-memory buffers also allow).  The default launches (mixed
-// window variant, FP64 direct loads) do not spill; within this budget the
-// ECG variants spill 16 bytes per thread, the FP64 window variant 32 and
-// the generic kernels (run-time fit shapes) 16-116 (ptxas -v).
+// bulk-staged, FP64 direct loads) do not spill; within this budget the
+// mixed window variant spills 4-12 bytes per thread, the mixed ECG
+// variants 4, the FP64 window variant 32 and the generic kernels (run-time
+// fit shapes) 12-116 (ptxas -v).
 #ifndef CDB_FP64_MIN_CTAS
 #define CDB_FP64_MIN_CTAS 4
 #endif

@@ -9,6 +9,7 @@ Tolerances (written here, checked below):
 """
 import numpy as np
 import pytest
+import torch
 
 from cardioid_b200 import engine as eng_mod
 from cardioid_b200 import tissue, tt06
@@ -166,13 +167,26 @@ def test_step_host_equals_device_step(cdb_lib, fits002):
         np.testing.assert_array_equal(vm, ref)
 
 
-@pytest.mark.parametrize("kind,precision", [("box", "fp64"), ("box", "mixed"), ("sheet", "mixed"),
-                                            ("masked", "fp64")])
-def test_chunked_step_host_equals_device_steps(cdb_lib, fits002, kind, precision):
+def _host_pair(vm0, locked):
+    """Two host Vm buffers, the first holding vm0: plain numpy arrays, or
+    page-locked ones (the chunked host step then replays captured graphs)."""
+    if not locked:
+        return np.ascontiguousarray(vm0, dtype=np.float64), np.empty(len(vm0))
+    a, b = (torch.empty(len(vm0), dtype=torch.float64, pin_memory=True) for _ in range(2))
+    a.numpy()[:] = vm0
+    return a.numpy(), b.numpy()
+
+
+@pytest.mark.parametrize("kind,precision,host", [("box", "fp64", "pageable"), ("box", "mixed", "pageable"),
+                                                 ("sheet", "mixed", "pageable"), ("masked", "fp64", "pageable"),
+                                                 ("box", "mixed", "locked"), ("masked", "fp64", "locked")])
+def test_chunked_step_host_equals_device_steps(cdb_lib, fits002, kind, precision, host):
     """cdb_engine_step_host on tissues large enough for its chunked pipeline
     (64^3 box: 4 chunks of z-planes; a 512 x 256 sheet: 8 chunks of rows; a
     masked box: 2 chunks): Vm, activation times and states bit-identical to
-    device-resident steps, across the stimulus and the wave it starts."""
+    device-resident steps, across the stimulus and the wave it starts; with
+    page-locked buffers through the two captured graphs of the alternating
+    buffer pair (the same kernels launched per step as issued directly)."""
     t = {"box": lambda: tissue.box(64, 64, 64), "sheet": lambda: tissue.box(512, 256, 1),
          "masked": lambda: _masked(64, 48, 40)}[kind]()
     steps = 120
@@ -180,12 +194,14 @@ def test_chunked_step_host_equals_device_steps(cdb_lib, fits002, kind, precision
         tid = e.add_tissue(t, _reaction_ids(t))
         e.step(steps)
         ref = (e.read_vm(tid), e.read_activation(tid), e.read_states(tid))
+    per_step = []
     with _engine(fits002, precision) as e:
         tid = e.add_tissue(t, _reaction_ids(t))
-        vm = np.ascontiguousarray(t.vm0, dtype=np.float64)
-        out = np.empty_like(vm)
+        vm, out = _host_pair(t.vm0, host == "locked")
         for _ in range(steps):
+            before = e.launch_count()
             e.step_host(tid, vm, out)
+            per_step.append(e.launch_count() - before)
             vm, out = out, vm
         np.testing.assert_array_equal(vm, ref[0])
         np.testing.assert_array_equal(e.read_vm(tid), ref[0])
@@ -193,6 +209,36 @@ def test_chunked_step_host_equals_device_steps(cdb_lib, fits002, kind, precision
         np.testing.assert_array_equal(e.read_states(tid), ref[2])
         assert e.time(tid)[0] == steps
     assert (ref[1] > 0).any()
+    assert len(set(per_step[1:])) == 1 and per_step[-1] > 3
+
+
+def test_host_step_graphs_follow_changes(cdb_lib, fits002):
+    """Captured host-step graphs are dropped when what they captured changes:
+    a retuned launch, a Vm written from the host and a second buffer pair
+    between host steps give the same Vm as device-resident steps with the
+    same changes."""
+    t = tissue.box(64, 64, 64)
+    vm_set = np.full(t.n, -20.0)
+    with _engine(fits002, "mixed") as e:
+        tid = e.add_tissue(t, _reaction_ids(t))
+        e.step(30)
+        e.set_tuning(0, 0)
+        e.step(30)
+        e.write_vm(tid, vm_set)
+        e.step(30)
+        ref = e.read_vm(tid)
+    with _engine(fits002, "mixed") as e:
+        tid = e.add_tissue(t, _reaction_ids(t))
+        vm, out = _host_pair(t.vm0, True)
+        for k in range(90):
+            if k == 30:
+                e.set_tuning(0, 0)
+            if k == 60:
+                vm2, out = _host_pair(vm_set, True)
+                vm = vm2
+            e.step_host(tid, vm, out)
+            vm, out = out, vm
+        np.testing.assert_array_equal(vm, ref)
 
 
 @pytest.mark.parametrize("graphs", [True, False])
