@@ -279,8 +279,9 @@ cdb_status cdb_engine_read_weights(cdb_engine* e, int32_t id, double* host19);
  * order (non-decreasing gid) and it has at least 32 planes along its
  * slowest axis and 65536 cells, the step runs in chunks of planes so the
  * upload, the step and the download overlap (both copy directions need
- * page-locked host buffers to overlap); vm_in and vm_out may be the same
- * buffer. */
+ * page-locked host buffers to overlap; with page-locked buffers the chunked
+ * step is captured once per (vm_in, vm_out, Vm parity) as a CUDA graph and
+ * replayed); vm_in and vm_out may be the same buffer. */
 cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, double* vm_out);
 /* ------------------------------------------------------------------ */
 /* Diagnostics                                                           */

@@ -212,6 +212,23 @@ def test_chunked_step_host_equals_device_steps(cdb_lib, fits002, kind, precision
     assert len(set(per_step[1:])) == 1 and per_step[-1] > 3
 
 
+@pytest.mark.parametrize("host", ["pageable", "locked"])
+def test_chunked_step_host_in_place(cdb_lib, fits002, host):
+    """vm_in and vm_out may be one buffer: each output range goes down only
+    after every chunk it overlaps has gone up."""
+    t = tissue.box(64, 64, 64)
+    with _engine(fits002, "mixed") as e:
+        tid = e.add_tissue(t, _reaction_ids(t))
+        e.step(40)
+        ref = e.read_vm(tid)
+    with _engine(fits002, "mixed") as e:
+        tid = e.add_tissue(t, _reaction_ids(t))
+        vm, _ = _host_pair(t.vm0, host == "locked")
+        for _ in range(40):
+            e.step_host(tid, vm, vm)
+        np.testing.assert_array_equal(vm, ref)
+
+
 def test_host_step_graphs_follow_changes(cdb_lib, fits002):
     """Captured host-step graphs are dropped when what they captured changes:
     a retuned launch, a Vm written from the host and a second buffer pair
