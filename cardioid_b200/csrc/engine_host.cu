@@ -1531,8 +1531,8 @@ cdb_status cdb_engine_step_host(cdb_engine* e, int32_t id, const double* vm_in, 
   // overlap, and every kernel stays on the engine's stream (the persistent
   // step kernels hold every SM while they run).  With page-locked host
   // buffers the whole pattern (about ten API calls per chunk) is captured
-  // once as a graph and replayed by one launch, so the copies are queued at
-  // once instead of behind the host's issue of the chunks before them.
+  // once as a graph and replayed by one launch: the same device time, and
+  // the host thread issues one call per step instead of some 170.
   cdb_status st = E.ensure_times(1);
   if (st != CDB_OK) return st;
   st = E.rebuild();
