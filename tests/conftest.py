@@ -7,6 +7,14 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
+# Under pytest-xdist every worker would start one OpenMP thread per core in
+# the reference build and the oracle; their spinning threads then slow the
+# suite from minutes to a quarter of an hour.  Each worker takes its share
+# of the cores instead (set before either library loads).
+if os.environ.get("PYTEST_XDIST_WORKER") and "OMP_NUM_THREADS" not in os.environ:
+    _workers = max(1, int(os.environ.get("PYTEST_XDIST_WORKER_COUNT", "1")))
+    os.environ["OMP_NUM_THREADS"] = str(max(1, (os.cpu_count() or 1) // _workers))
+
 
 
 def reference_root():
