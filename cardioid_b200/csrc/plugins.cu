@@ -189,9 +189,12 @@ cdb_status cdb_reaction_create(int device, cdb_precision precision, const cdb_tt
 
 cdb_status cdb_reaction_init(cdb_reaction* r, const int32_t* indexArray, double* Vm, void* stream)
 {
-  CDB_CHECK(r && indexArray && Vm, CDB_INVALID_ARG, "null argument");
-  CDB_CUDA(cudaSetDevice(r->device));
+  CDB_CHECK(r, CDB_INVALID_ARG, "null argument");
+  // a reaction with no cells (its cellTypes absent from the tissue) has
+  // nothing to do, whatever its (possibly null, empty) arrays
   if (r->n == 0) return CDB_OK;
+  CDB_CHECK(indexArray && Vm, CDB_INVALID_ARG, "null argument");
+  CDB_CUDA(cudaSetDevice(r->device));
   reaction_init_kernel<<<(unsigned)((r->n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
       r->n, r->s64.as<double>(), r->s32.as<float>(), r->prec == CDB_MIXED, indexArray, Vm);
   CDB_CUDA(cudaGetLastError());
@@ -202,10 +205,11 @@ cdb_status cdb_reaction_calc(cdb_reaction* r, double dt, const int32_t* indexArr
                              const double* iStim, double* dVm, void* stream)
 {
   (void)iStim;   // unused by BetterTT06::calc, as in the reference (elec/BetterTT06.cc:1429)
-  CDB_CHECK(r && indexArray && Vm && dVm, CDB_INVALID_ARG, "null argument");
+  CDB_CHECK(r, CDB_INVALID_ARG, "null argument");
   CDB_CHECK(dt == r->dt, CDB_INVALID_ARG, "dt differs from the dt the fits were made for");
+  if (r->n == 0) return CDB_OK;   // no cells: nothing to read or write (arrays may be null)
+  CDB_CHECK(indexArray && Vm && dVm, CDB_INVALID_ARG, "null argument");
   CDB_CUDA(cudaSetDevice(r->device));
-  if (r->n == 0) return CDB_OK;
   if (r->slot >= 0) {
     CDB_CUDA(reaction_slot_calc(r->slot, r->prec == CDB_MIXED, r->n, dt, indexArray, Vm, dVm, r->s64.as<double>(),
                                 r->s32.as<float>(), (cudaStream_t)stream));
@@ -230,8 +234,10 @@ cdb_status cdb_reaction_calc(cdb_reaction* r, double dt, const int32_t* indexArr
 
 cdb_status cdb_reaction_get_state(cdb_reaction* r, int var, double* host)
 {
-  CDB_CHECK(r && host, CDB_INVALID_ARG, "null argument");
+  CDB_CHECK(r, CDB_INVALID_ARG, "null argument");
   CDB_CHECK(var >= 0 && var < kNumStates, CDB_INVALID_ARG, "state index out of range");
+  if (r->n == 0) return CDB_OK;
+  CDB_CHECK(host, CDB_INVALID_ARG, "null argument");
   CDB_CUDA(cudaSetDevice(r->device));
   CDB_CUDA(cudaDeviceSynchronize());
   const int64_t n = r->n;
@@ -247,8 +253,10 @@ cdb_status cdb_reaction_get_state(cdb_reaction* r, int var, double* host)
 
 cdb_status cdb_reaction_set_state(cdb_reaction* r, int var, const double* host)
 {
-  CDB_CHECK(r && host, CDB_INVALID_ARG, "null argument");
+  CDB_CHECK(r, CDB_INVALID_ARG, "null argument");
   CDB_CHECK(var >= 0 && var < kNumStates, CDB_INVALID_ARG, "state index out of range");
+  if (r->n == 0) return CDB_OK;
+  CDB_CHECK(host, CDB_INVALID_ARG, "null argument");
   CDB_CUDA(cudaSetDevice(r->device));
   CDB_CUDA(cudaDeviceSynchronize());
   const int64_t n = r->n;

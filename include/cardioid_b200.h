@@ -114,7 +114,10 @@ cdb_status cdb_reaction_create(int device, cdb_precision precision, const cdb_tt
 cdb_status cdb_reaction_init(cdb_reaction* r, const int32_t* indexArray, double* Vm, void* stream);
 /* dVm[indexArray[i]] = -Iion(Vm[indexArray[i]], state_i); state advanced
  * by dt.  iStim is accepted and unused, as in the reference.  All device
- * pointers; stream is a cudaStream_t (NULL = default stream). */
+ * pointers; stream is a cudaStream_t (NULL = default stream).  A reaction
+ * created with nCells = 0 (a REACTION whose cellTypes the tissue lacks, as
+ * ReactionManager::create can make) returns CDB_OK from init and calc
+ * without touching its arrays, which may then be NULL. */
 cdb_status cdb_reaction_calc(cdb_reaction* r, double dt, const int32_t* indexArray, const double* Vm,
                              const double* iStim, double* dVm, void* stream);
 /* var in checkpoint order (Ca_SR Ca_i Ca_ss K_i Na_i R_prime Xr1 Xr2 Xs d f

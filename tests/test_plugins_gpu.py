@@ -54,13 +54,12 @@ def test_fgr_plugin_matches_oracle_weights_and_dvm(cdb_lib, oracle_port, fits002
     assert np.abs(dVm.cpu().numpy() - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
 
 
-def test_split_plugins_loop_matches_oracle(cdb_lib, oracle_port, fits002):
-    """ReactionManager + FGRDiffusion + stimulus + integrator, step by step
-    as the omp loop, for 300 steps: within the FP64 parity tolerance
-    (1e-6 mV) of the oracle."""
+def _split_loop(t, steps):
+    """The omp loop's step order on the drop-in plugins (ReactionManager over
+    the three declared reactions, FGR diffusion, box stimulus, integrator);
+    returns the final Vm and the reaction manager."""
     import torch
     from cardioid_b200 import engine
-    t = tissue.box(10, 8, 6)
     db = objectdb.ObjectDB()
     for ct in (0, 1, 2):
         db.compile_file(engine.shipped_fit_path(DT, ct))
@@ -68,7 +67,6 @@ def test_split_plugins_loop_matches_oracle(cdb_lib, oracle_port, fits002):
     db.compile("fgr DIFFUSION { method = FGR; diffusionScale = %r; }" % t.diffusion_scale)
     rm = plugins.ReactionManager(db, ["tt06Endo", "tt06Mid", "tt06Epi"], DT, t.cell_type)
     diff = plugins.diffusionFactory(db, "fgr", t)
-    sim = oracle_port.PortSim(t, fits002, (t.cell_type - 100).astype(np.uint8), DT)
     x, y, z = t.tuples()
     s = t.stimuli[0]
     inbox = torch.from_numpy((x > s.xMin) & (x < s.xMax) & (y > s.yMin) & (y < s.yMax) & (z > s.zMin) &
@@ -77,7 +75,7 @@ def test_split_plugins_loop_matches_oracle(cdb_lib, oracle_port, fits002):
     dVmR, dVmD = torch.zeros_like(Vm), torch.zeros_like(Vm)
     iStim = torch.zeros_like(Vm)
     time = 0.0
-    for _ in range(300):
+    for _ in range(steps):
         iStim.zero_()
         v = s.value(time)
         if v != 0:
@@ -87,8 +85,46 @@ def test_split_plugins_loop_matches_oracle(cdb_lib, oracle_port, fits002):
         diff.calc(dVmD)
         Vm += DT * (dVmR + dVmD + iStim)
         time += DT
+    return Vm.cpu().numpy(), rm
+
+
+def test_split_plugins_loop_matches_oracle(cdb_lib, oracle_port, fits002):
+    """ReactionManager + FGRDiffusion + stimulus + integrator, step by step
+    as the omp loop, for 300 steps: within the FP64 parity tolerance
+    (1e-6 mV) of the oracle."""
+    t = tissue.box(10, 8, 6)
+    vm, _ = _split_loop(t, 300)
+    sim = oracle_port.PortSim(t, fits002, (t.cell_type - 100).astype(np.uint8), DT)
     sim.step(300)
-    assert np.abs(Vm.cpu().numpy() - sim.vm()).max() <= 1e-6
+    assert np.abs(vm - sim.vm()).max() <= 1e-6
+
+
+def test_reaction_without_cells_is_a_no_op(cdb_lib, oracle_port, fits002):
+    """A declared REACTION whose cellTypes the tissue lacks (here the mid
+    type: its cells made endo) is created with no cells, as
+    ReactionManager::create does; its init and calc return without touching
+    anything, even with empty (null) arrays, and the loop over the other two
+    matches the oracle (1e-6 mV after 200 steps)."""
+    import torch
+    t = tissue.box(10, 8, 6)
+    t.cell_type[t.cell_type == 101] = 100
+    vm, rm = _split_loop(t, 200)
+    assert [r.nCells for r in rm.reactions] == [int((t.cell_type == 100).sum()), 0, int((t.cell_type == 102).sum())]
+    sim = oracle_port.PortSim(t, fits002, (t.cell_type - 100).astype(np.uint8), DT)
+    sim.step(200)
+    assert np.abs(vm - sim.vm()).max() <= 1e-6
+    empty = rm.reactions[1]
+    idx = torch.zeros(0, dtype=torch.int32, device="cuda")
+    Vm = torch.zeros(0, dtype=torch.float64, device="cuda")
+    empty.calc(DT, idx, Vm, Vm, Vm)
+    empty.initializeMembraneVoltage(idx, Vm)
+    # the same through the real arrays of the loop: dVm keeps its NaNs
+    Vm = torch.from_numpy(vm).cuda()
+    dVm = torch.full_like(Vm, float("nan"))
+    empty.calc(DT, idx, Vm, torch.zeros_like(Vm), dVm)
+    torch.cuda.synchronize()
+    assert bool(torch.isnan(dVm).all())
+    assert empty.getValues(0).shape == (0,)
 
 
 def _single_type(n, vm):
