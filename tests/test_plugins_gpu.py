@@ -38,9 +38,25 @@ def test_reaction_plugin_index_gather_scatter(cdb_lib, oracle_port, fits002):
         np.testing.assert_allclose(ours, st[k][perm], rtol=1e-9, atol=1e-15)
 
 
-def test_fgr_plugin_matches_oracle_weights_and_dvm(cdb_lib, oracle_port, fits002):
+def _masked_box(nx, ny, nz):
+    """A box with a hole through its middle and one missing edge column."""
+    full = tissue.box(nx, ny, nz)
+    x, y, z = full.tuples()
+    keep = ~((x >= nx // 3) & (x < 2 * nx // 3) & (y >= ny // 3) & (y < 2 * ny // 3))
+    keep &= ~((x == nx - 1) & (y == 0))
+    return tissue.Tissue(full.nx, full.ny, full.nz, full.dx, full.dy, full.dz, full.gid[keep], full.cell_type[keep],
+                         full.sigma[keep], full.vm0[keep], full.stimuli)
+
+
+@pytest.mark.parametrize("kind", ["box", "cable", "sheet", "masked"])
+def test_fgr_plugin_matches_oracle_weights_and_dvm(cdb_lib, oracle_port, fits002, kind):
+    """FGRDiffusion's 19 weights bit for bit and its dVm within 1e-12 of the
+    largest |dVm| against the oracle, on a box, a cable and a sheet (the
+    missing neighbours get no weight) and a box with a hole (no-flux faces
+    inside the grid)."""
     import torch
-    t = tissue.box(11, 9, 7)
+    t = {"box": lambda: tissue.box(11, 9, 7), "cable": lambda: tissue.box(40, 1, 1),
+         "sheet": lambda: tissue.box(20, 16, 1), "masked": lambda: _masked_box(12, 11, 9)}[kind]()
     d = plugins.FGRDiffusion(t)
     sim = oracle_port.PortSim(t, fits002, (t.cell_type - 100).astype(np.uint8), DT)
     np.testing.assert_array_equal(d.weights(), sim.weights())
@@ -54,10 +70,12 @@ def test_fgr_plugin_matches_oracle_weights_and_dvm(cdb_lib, oracle_port, fits002
     assert np.abs(dVm.cpu().numpy() - ref).max() <= 1e-12 * max(1.0, np.abs(ref).max())
 
 
-def _split_loop(t, steps):
+def _split_loop(t, steps, precision="fp64", probes=None, every=10):
     """The omp loop's step order on the drop-in plugins (ReactionManager over
-    the three declared reactions, FGR diffusion, box stimulus, integrator);
-    returns the final Vm and the reaction manager."""
+    the three declared reactions, FGR diffusion, box stimulus, integrator).
+    Returns the final Vm, the reaction manager, the activation times (first
+    post-step time with Vm > 0, -1 if none) and, with probes, their Vm and
+    the time every `every` steps."""
     import torch
     from cardioid_b200 import engine
     db = objectdb.ObjectDB()
@@ -65,7 +83,7 @@ def _split_loop(t, steps):
         db.compile_file(engine.shipped_fit_path(DT, ct))
     db.compile(tissue.reaction_objects_text(["tt06Endo_fit", "tt06Mid_fit", "tt06Epi_fit"]))
     db.compile("fgr DIFFUSION { method = FGR; diffusionScale = %r; }" % t.diffusion_scale)
-    rm = plugins.ReactionManager(db, ["tt06Endo", "tt06Mid", "tt06Epi"], DT, t.cell_type)
+    rm = plugins.ReactionManager(db, ["tt06Endo", "tt06Mid", "tt06Epi"], DT, t.cell_type, precision=precision)
     diff = plugins.diffusionFactory(db, "fgr", t)
     x, y, z = t.tuples()
     s = t.stimuli[0]
@@ -74,8 +92,10 @@ def _split_loop(t, steps):
     Vm = torch.from_numpy(t.vm0.copy()).cuda()
     dVmR, dVmD = torch.zeros_like(Vm), torch.zeros_like(Vm)
     iStim = torch.zeros_like(Vm)
+    act = torch.full_like(Vm, -1.0)
+    trace, times = [], []
     time = 0.0
-    for _ in range(steps):
+    for k in range(steps):
         iStim.zero_()
         v = s.value(time)
         if v != 0:
@@ -85,7 +105,12 @@ def _split_loop(t, steps):
         diff.calc(dVmD)
         Vm += DT * (dVmR + dVmD + iStim)
         time += DT
-    return Vm.cpu().numpy(), rm
+        act = torch.where((act < 0) & (Vm > 0), torch.full_like(act, time), act)
+        if probes is not None and (k + 1) % every == 0:
+            trace.append(Vm[probes].cpu().numpy())
+            times.append(time)
+    out = (Vm.cpu().numpy(), rm, act.cpu().numpy())
+    return out + ((np.array(trace), np.array(times)) if probes is not None else ())
 
 
 def test_split_plugins_loop_matches_oracle(cdb_lib, oracle_port, fits002):
@@ -93,10 +118,35 @@ def test_split_plugins_loop_matches_oracle(cdb_lib, oracle_port, fits002):
     as the omp loop, for 300 steps: within the FP64 parity tolerance
     (1e-6 mV) of the oracle."""
     t = tissue.box(10, 8, 6)
-    vm, _ = _split_loop(t, 300)
+    vm, _, _ = _split_loop(t, 300)
     sim = oracle_port.PortSim(t, fits002, (t.cell_type - 100).astype(np.uint8), DT)
     sim.step(300)
     assert np.abs(vm - sim.vm()).max() <= 1e-6
+
+
+def test_mixed_reaction_plugins_vs_fp64_oracle(cdb_lib, oracle_port, fits002):
+    """The split loop with the mixed-precision plugin reactions (FP64 FGR
+    diffusion) on a 12x10x8 box for 20000 steps (400 ms, one paced beat)
+    against the FP64 oracle: every cell activates, activation times within
+    0.5 ms, APD90 within 1 ms at probe cells (the mixed path's tolerances)."""
+    from cardioid_b200.sensors import apd90
+    t = tissue.box(12, 10, 8, period=1000.0)
+    probes = np.array([0, 7, t.n // 3, t.n // 2, t.n - 1])
+    steps, every = 20000, 10
+    _, _, act_m, tr_m, times = _split_loop(t, steps, "mixed", probes, every)
+    sim = oracle_port.PortSim(t, fits002, (t.cell_type - 100).astype(np.uint8), DT)
+    tr_o = []
+    for _ in range(0, steps, every):
+        sim.step(every)
+        tr_o.append(sim.vm()[probes])
+    tr_o = np.array(tr_o)
+    act_o = sim.activation()
+    assert (act_o > 0).all() and (act_m > 0).all()
+    assert np.abs(act_m - act_o).max() <= 0.5
+    for j in range(len(probes)):
+        a_o, a_m = apd90(tr_o[:, j], times), apd90(tr_m[:, j], times)
+        assert len(a_o) == len(a_m) and len(a_o) >= 1
+        assert np.abs(a_o - a_m).max() <= 1.0
 
 
 def test_reaction_without_cells_is_a_no_op(cdb_lib, oracle_port, fits002):
@@ -108,7 +158,7 @@ def test_reaction_without_cells_is_a_no_op(cdb_lib, oracle_port, fits002):
     import torch
     t = tissue.box(10, 8, 6)
     t.cell_type[t.cell_type == 101] = 100
-    vm, rm = _split_loop(t, 200)
+    vm, rm, _ = _split_loop(t, 200)
     assert [r.nCells for r in rm.reactions] == [int((t.cell_type == 100).sum()), 0, int((t.cell_type == 102).sum())]
     sim = oracle_port.PortSim(t, fits002, (t.cell_type - 100).astype(np.uint8), DT)
     sim.step(200)
