@@ -54,6 +54,48 @@ def test_adapter_in_reference_reaction_manager(cdb_lib):
         assert np.abs(gpu.state(name) - r).max() <= 1e-8 * max(1e-12, np.abs(r).max())
 
 
+@pytest.mark.skipif(not _built(), reason="oracle/_ref with the adapter not built")
+def test_mixed_adapter_in_reference_loop_over_one_beat(cdb_lib):
+    """REACTION objects with precision = mixed: the adapter's mixed-precision
+    reactions inside the reference's time loop for one paced beat (20000
+    steps, 400 ms) against the reference's own BetterTT06 (FP64): every cell
+    activates in both, activation times within 0.5 ms, APD90 within 1 ms at
+    probe cells (the mixed path's tolerances)."""
+    from golden.make_golden import reference_sim
+    from oracle import refsim
+    from cardioid_b200.sensors import apd90
+    t = tissue.box(10, 8, 6, dx=0.2, seed=29)
+    ref = reference_sim(t)
+    text = ""
+    for name, ct, fit in (("b200mEndo", 0, "tt06Endo_fit"), ("b200mMid", 1, "tt06Mid_fit"),
+                          ("b200mEpi", 2, "tt06Epi_fit")):
+        text += "%s REACTION { method = %s; cellTypes = %d; celltype = %d; fit = %s; precision = mixed; }\n" % (
+            name, ADAPTER, 100 + ct, ct, fit)
+    refsim.compile_once("b200-adapter-mixed", text)
+    prefix = refsim.unique_prefix()
+    refsim.compile_objects(tissue.stimulus_objects_text(t.stimuli, prefix=prefix))
+    gpu = refsim.RefSim(["b200mEndo", "b200mMid", "b200mEpi"], ["%s%d" % (prefix, i) for i in range(len(t.stimuli))],
+                        (t.nx, t.ny, t.nz), (t.dx, t.dy, t.dz), t.gid, t.cell_type, t.sigma, 0.02, t.diffusion_scale)
+    ref.set_vm(t.vm0)
+    gpu.set_vm(t.vm0)
+    probes = np.array([0, 9, t.n // 2, t.n - 1])
+    tr_r, tr_g, times = [], [], []
+    for _ in range(2000):
+        ref.step(10)
+        gpu.step(10)
+        tr_r.append(ref.vm()[probes])
+        tr_g.append(gpu.vm()[probes])
+        times.append(ref.time)
+    act_r, act_g = ref.activation(), gpu.activation()
+    assert (act_r > 0).all() and (act_g > 0).all()
+    assert np.abs(act_g - act_r).max() <= 0.5
+    tr_r, tr_g, times = np.array(tr_r), np.array(tr_g), np.array(times)
+    for j in range(len(probes)):
+        a_r, a_g = apd90(tr_r[:, j], times), apd90(tr_g[:, j], times)
+        assert len(a_r) == len(a_g) and len(a_r) >= 1
+        assert np.abs(a_r - a_g).max() <= 1.0
+
+
 FGR_ADAPTER = os.path.join(ROOT, "oracle", "_ref", "libb200fgr.so")
 
 
