@@ -99,19 +99,21 @@ def test_config0_fp64_parity_64cubed_1000_steps(cdb_lib, oracle_port, fits002):
     assert (act > 0).sum() > t.n // 4
 
 
-def test_batched_tissues_equal_alone(cdb_lib, fits002):
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_tissues_equal_alone(cdb_lib, fits002, precision):
     """Index handling: tissues packed into one launch give bit-identical
-    results to each tissue run alone, per-tissue drug block included."""
+    results to each tissue run alone, per-tissue drug block included, in
+    both precisions."""
     ts = [tissue.box(20, 1, 1, seed=1), tissue.box(10, 9, 1, seed=2), tissue.box(7, 6, 5, seed=3),
           _masked(9, 8, 7, seed=4)]
     scales = [(1.0, 1.0, 1.0), (0.5, 1.0, 1.0), (1.0, 0.3, 0.8), (0.2, 0.9, 0.1)]
     alone = []
     for t, sc in zip(ts, scales):
-        with _engine(fits002) as e:
+        with _engine(fits002, precision) as e:
             tid = e.add_tissue(t, _reaction_ids(t), sc)
             e.step(300)
             alone.append((e.read_vm(tid), e.read_states(tid), e.read_activation(tid)))
-    with _engine(fits002) as e:
+    with _engine(fits002, precision) as e:
         ids = [e.add_tissue(t, _reaction_ids(t), sc) for t, sc in zip(ts, scales)]
         e.step(300)
         for tid, (vm, st, act) in zip(ids, alone):

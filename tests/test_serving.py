@@ -169,18 +169,21 @@ def test_partition_over_two_gloo_ranks_serves_every_job_once():
 
 
 @pytest.mark.gpu
-def test_served_job_equals_job_alone(cdb_lib, fits002):
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_served_job_equals_job_alone(cdb_lib, fits002, precision):
+    """A job served among others (joining and retiring between batches)
+    activates bit for bit as the same job run alone, in both precisions."""
     from cardioid_b200 import engine as eng_mod
     spec = serving.JobSpec(rate=1e6, median_cells=2000, sigma=0.8, max_cells=20000, steps=700,
                            population=pop.PopulationSpec(cl=(5.0, 12.0)))
     jobs = serving.draw_jobs(8, spec, seed=3)
-    with eng_mod.Engine(0.02, precision="fp64") as e:
+    with eng_mod.Engine(0.02, precision=precision) as e:
         rid = [e.add_reaction(p) for p in fits002]
         res = serving.Server(e, rid, batch=150, keep=True, reserve=0).run(jobs)
     assert len(res) == len(jobs)
     for r in res[:3]:
         inst = jobs[r.id].instance
-        with eng_mod.Engine(0.02, precision="fp64") as e:
+        with eng_mod.Engine(0.02, precision=precision) as e:
             rid = [e.add_reaction(p) for p in fits002]
             t = pop.build(inst)
             tid = e.add_tissue(t, np.full(t.n, rid[inst.celltype], np.uint8), scales=inst.scales)
