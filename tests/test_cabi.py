@@ -55,3 +55,21 @@ def test_bad_config_is_rejected_before_touching_a_device(cdb_lib):
     h = ctypes.c_void_p()
     assert cdb_lib.cdb_engine_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.CDB_INVALID_ARG
     assert b"dt" in cdb_lib.cdb_last_error()
+
+
+def test_static_stencil_checks_its_arguments_before_touching_a_device(cdb_lib):
+    """cdb_fgr_calc_static rejects, on the host and before any CUDA call,
+    null pointers, empty grids, a bad device index and boxes whose padded
+    block exceeds its static block of 2^21 voxels (the pointers below are
+    never dereferenced)."""
+    buf = (ctypes.c_double * 1)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    calc = cdb_lib.cdb_fgr_calc_static
+    assert calc(0, 4, 4, 4, None, p, p, 1.0, None) == _lib.CDB_INVALID_ARG
+    assert b"null" in cdb_lib.cdb_last_error()
+    assert calc(0, 0, 4, 4, p, p, p, 1.0, None) == _lib.CDB_INVALID_ARG
+    assert calc(-1, 4, 4, 4, p, p, p, 1.0, None) == _lib.CDB_INVALID_ARG
+    # 126^3 fits exactly ((126 + 2)^3 = 2^21); one more voxel row does not
+    assert calc(0, 127, 126, 126, p, p, p, 1.0, None) == _lib.CDB_INVALID_ARG
+    assert b"static block" in cdb_lib.cdb_last_error()
+    assert calc(0, 200, 200, 200, p, p, p, 1.0, None) == _lib.CDB_INVALID_ARG
