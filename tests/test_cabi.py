@@ -73,3 +73,41 @@ def test_static_stencil_checks_its_arguments_before_touching_a_device(cdb_lib):
     assert calc(0, 127, 126, 126, p, p, p, 1.0, None) == _lib.CDB_INVALID_ARG
     assert b"static block" in cdb_lib.cdb_last_error()
     assert calc(0, 200, 200, 200, p, p, p, 1.0, None) == _lib.CDB_INVALID_ARG
+
+
+def test_plugin_create_checks_its_arguments_before_touching_a_device(cdb_lib):
+    """cdb_fgr_create and cdb_diff6_create reject an empty or bad grid, a
+    cell count outside 1..nx*ny*nz and a gid outside the grid, and
+    cdb_reaction_create a negative cell count, a bad dt or an unknown
+    precision, all on the host before any CUDA call."""
+    gid = np.array([0, 5, 60], dtype=np.int64)
+    ct = np.full(3, 100, dtype=np.int32)
+    sig = np.zeros((3, 6))
+    h = ctypes.c_void_p()
+
+    def fgr(nx, ny, nz, n, g=gid):
+        return cdb_lib.cdb_fgr_create(0, nx, ny, nz, 0.2, 0.2, 0.2, n, g.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), ct.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                      _lib.dptr(sig), 1.0, ctypes.byref(h))
+
+    def diff6(nx, ny, nz, n, g=gid):
+        return cdb_lib.cdb_diff6_create(0, nx, ny, nz, 0.2, 0.2, 0.2, n, g.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _lib.dptr(sig), 1.0,
+                                        ctypes.byref(h))
+
+    for create in (fgr, diff6):
+        assert create(0, 4, 4, 3) == _lib.CDB_INVALID_ARG            # empty grid
+        assert create(4, 4, 4, 0) == _lib.CDB_INVALID_ARG            # no cells
+        assert create(2, 2, 2, 9) == _lib.CDB_INVALID_ARG            # more cells than voxels
+        assert create(4, 4, 3, 3) == _lib.CDB_INVALID_ARG            # gid 60 outside 4x4x3
+        assert b"gid" in cdb_lib.cdb_last_error()
+        assert create(4, 4, 4, 3, np.array([0, -1, 2], dtype=np.int64)) == _lib.CDB_INVALID_ARG
+    assert h.value is None
+    from cardioid_b200 import engine
+    p = engine.default_params(0, 0.02)
+    cp = _lib.to_params(p)
+    fits = _lib.to_fit_array(p.fits)
+    assert cdb_lib.cdb_reaction_create(0, 0, ctypes.byref(cp), fits, -1, 0.02, ctypes.byref(h)) == _lib.CDB_INVALID_ARG
+    assert cdb_lib.cdb_reaction_create(0, 0, ctypes.byref(cp), fits, 10, 0.0, ctypes.byref(h)) == _lib.CDB_INVALID_ARG
+    assert b"dt" in cdb_lib.cdb_last_error()
+    assert cdb_lib.cdb_reaction_create(0, 7, ctypes.byref(cp), fits, 10, 0.02, ctypes.byref(h)) == _lib.CDB_INVALID_ARG
+    assert b"precision" in cdb_lib.cdb_last_error()
+    assert h.value is None
