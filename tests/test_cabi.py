@@ -111,3 +111,30 @@ def test_plugin_create_checks_its_arguments_before_touching_a_device(cdb_lib):
     assert cdb_lib.cdb_reaction_create(0, 7, ctypes.byref(cp), fits, 10, 0.02, ctypes.byref(h)) == _lib.CDB_INVALID_ARG
     assert b"precision" in cdb_lib.cdb_last_error()
     assert h.value is None
+
+
+def test_unknown_precision_is_rejected_before_touching_a_device(cdb_lib):
+    cfg = _lib.EngineConfig()
+    cfg.dt, cfg.precision = 0.02, 5
+    h = ctypes.c_void_p()
+    assert cdb_lib.cdb_engine_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.CDB_INVALID_ARG
+    assert b"precision" in cdb_lib.cdb_last_error()
+
+
+def test_engine_without_a_gpu_fails_loudly():
+    """With no CUDA device the engine does not fall back to anything: the C
+    ABI returns CDB_CUDA_ERROR with the CUDA runtime's message and the
+    Python engine raises."""
+    import pytest
+    from conftest import has_gpu
+    if has_gpu():
+        pytest.skip("a GPU is present")
+    from cardioid_b200 import engine
+    cfg = _lib.EngineConfig()
+    cfg.dt, cfg.precision = 0.02, 1
+    h = ctypes.c_void_p()
+    assert _lib.load().cdb_engine_create(ctypes.byref(cfg), ctypes.byref(h)) == _lib.CDB_CUDA_ERROR
+    assert _lib.load().cdb_last_error()
+    assert h.value is None
+    with pytest.raises(_lib.CdbError):
+        engine.Engine(0.02, precision="mixed")
